@@ -1,0 +1,388 @@
+"""Benchmark: T85 L60 round-trip spherical-harmonic transforms per second.
+
+Workload (config C1's grid and batch): T85 (256 lon x 128 Gauss lat), 60 levels
+x 8 fields = 480 field-levels, seeded spectra ~ (n+1)^-2 (seed 20261203; no
+dataset is involved).  One step = one round trip of the whole batch:
+xya_wa (spectral -> grid) then wa_xya (grid -> spectral).  A round-trip
+transform is one field-level through both.
+
+  value  device throughput with the spectra resident in HBM: field-level round
+         trips per second (CUDA events on the launching stream, L2 flushed with
+         a 256 MiB write between steps, outside the timed events).
+  e2e    the same metric through the host-pointer C-ABI (sht_xya_wa then
+         sht_wa_xya on pinned host arrays): every step moves the spectra in,
+         the grid out and back, and the spectra out over PCIe.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                        [--precision auto|fp64|split] [--nb NB]
+Under torchrun each rank runs the same batch on its own GPU (replicas: the
+transform of independent field-levels needs no exchange), the timing is the
+max over ranks and value is the total over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "T85L60 round-trip transforms/s: split-prec TC vs FP64 GPU, ≤1e-11 rel err"
+UNIT = "round-trip transforms/s"
+GRID = "T85"
+LEVELS, FIELDS, POWER = 60, 8, 2.0
+RADIUS = 6.371e6
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def _rel(a, b):
+    a = np.asarray(a).reshape(len(a), -1)
+    b = np.asarray(b).reshape(len(b), -1)
+    return float((np.abs(a - b).max(1) / np.abs(b).max(1)).max())
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = os.path.join("/tmp", f"clocks_{os.getpid()}.csv")
+
+    def start(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.close()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+# ------------------------------------------------------------- reference
+def run_reference(args):
+    """The reference's CPU transform (the oracle's restatement of SPMODEL's
+    w_xy/xy_w, OpenMP over field-levels as SpmlUtil does), all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W = importlib.import_module("dennou-ogcm_b200.workloads")
+    I, J, N = W.GRIDS[GRID]
+    nb = args.nb or LEVELS * FIELDS
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    p = O.OraclePlan(I, J, N, RADIUS)
+    w = W.seeded_spectra(N, nb, POWER)
+    for _ in range(args.warmup):
+        p.wa_xya(p.xya_wa(w))
+    t = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = p.wa_xya(p.xya_wa(w))
+        t.append(time.perf_counter() - t0)
+    tot = sum(t)
+    value = nb * args.steps / tot
+    rec = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic (seeded spectra, seed 20261203)",
+           "config": {"workload": f"{GRID} L{LEVELS} x {FIELDS} fields round trip (xy_w then w_xy)",
+                      "field_levels": nb, "im": I, "jm": J, "nm": N},
+           "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                            "sample": f"{args.steps} full steps of {nb} field-levels, OpenMP over field-levels"},
+           "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+           "roundtrip_relerr": _rel(out, w)}
+    print(json.dumps(rec))
+    return 0
+
+
+def cpu_baseline(nb, seconds=10.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    W = importlib.import_module("dennou-ogcm_b200.workloads")
+    I, J, N = W.GRIDS[GRID]
+    cores = os.cpu_count() or 1
+    O.set_threads(cores)
+    p = O.OraclePlan(I, J, N, RADIUS)
+    w = W.seeded_spectra(N, nb, POWER)
+    p.wa_xya(p.xya_wa(w))
+    done, t0 = 0, time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        p.wa_xya(p.xya_wa(w))
+        done += nb
+    el = time.perf_counter() - t0
+    return {"value": done / el, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{done} field-level round trips ({done // nb} batches of {nb}) in {el:.1f} s"}
+
+
+# ------------------------------------------------------------------ ours
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
+    ap.add_argument("--nb", type=int, default=0, help="field-levels (default 480)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=dev)
+
+    P = importlib.import_module("dennou-ogcm_b200")
+    W = importlib.import_module("dennou-ogcm_b200.workloads")
+    I, J, N = W.GRIDS[GRID]
+    nb = args.nb or LEVELS * FIELDS
+    L = (N + 1) ** 2
+    sht = P.SpmlUtil(I, J, LEVELS, N, None, RADIUS)
+    lib = P.load_library()
+    stream = torch.cuda.current_stream(dev)
+
+    w_in = W.seeded_spectra_torch(N, nb, POWER, dev)
+    grid = torch.empty((nb, J, I), dtype=torch.float64, device=dev)
+    w_out = torch.empty((nb, L), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 8, dtype=torch.float64, device=dev)
+    h = sht._h
+    VP = ctypes.c_void_p
+    lib.sht_set_stream(h, VP(stream.cuda_stream))
+
+    def step():
+        st = lib.sht_xya_wa_dev(h, VP(w_in.data_ptr()), nb, VP(grid.data_ptr()))
+        st |= lib.sht_wa_xya_dev(h, VP(grid.data_ptr()), nb, VP(w_out.data_ptr()))
+        if st:
+            raise RuntimeError(lib.sht_last_error().decode())
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(prec):
+        sht.set_precision(prec)
+        for _ in range(args.warmup):
+            flush.zero_()
+            step()
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        n0 = P.launch_count()
+        clk = ClockSampler(str(torch.cuda.get_device_properties(dev).uuid)
+                           if hasattr(torch.cuda.get_device_properties(dev), "uuid") else str(local))
+        clk.start()
+        evs = []
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            step()
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - wall0
+        barrier()
+        torch.cuda.synchronize()
+        clocks = clk.stop()
+        launches = P.launch_count() - n0
+        ms = [a.elapsed_time(b) for a, b in evs]
+        tot = max_over_ranks(sum(ms))
+        err = _rel(w_out.cpu().numpy(), w_in.cpu().numpy())
+        return {"value": world * nb * args.steps / (tot * 1e-3), "ms_per_step": tot / args.steps,
+                "launches": launches, "clocks": clocks, "relerr": err, "wall_s": wall}
+
+    # stage breakdown of one round trip for the roofline (separate pass, timing on)
+    def stages(prec):
+        sht.set_precision(prec)
+        sht.set_timing(True)
+        acc = {"syn": np.zeros(3), "ana": np.zeros(3)}
+        reps = 5
+        for _ in range(reps):
+            flush.zero_()
+            lib.sht_xya_wa_dev(h, VP(w_in.data_ptr()), nb, VP(grid.data_ptr()))
+            t = sht.last_timing()
+            acc["syn"] += [t["fft_ms"], t["legendre_ms"], t["spectral_ms"]]
+            flush.zero_()
+            lib.sht_wa_xya_dev(h, VP(grid.data_ptr()), nb, VP(w_out.data_ptr()))
+            t = sht.last_timing()
+            acc["ana"] += [t["fft_ms"], t["legendre_ms"], t["spectral_ms"]]
+        sht.set_timing(False)
+        return {k: (v / reps).tolist() for k, v in acc.items()}
+
+    results = {}
+    modes = ["fp64", "split"] if args.precision == "auto" else [args.precision]
+    for mode in modes:
+        prec = P.SHT_PREC_FP64 if mode == "fp64" else P.SHT_PREC_SPLIT
+        try:
+            results[mode] = timed(prec)
+            results[mode]["stages_ms"] = stages(prec)
+        except (P.SpmlError, RuntimeError) as ex:
+            results[mode] = {"error": str(ex)}
+    ok = {m: r for m, r in results.items() if "value" in r and r["relerr"] <= 1e-11}
+    head_mode = "split" if "split" in ok else ("fp64" if "fp64" in ok else None)
+    if head_mode is None:
+        raise SystemExit(f"no precision mode met 1e-11: {results}")
+    head = results[head_mode]
+
+    # roofline of the dominant kernel (largest share of the round trip)
+    peaks, pk_kind = _peaks()
+    fp64_dfma, fp64_dmma = ctypes.c_double(), ctypes.c_double()
+    lib.sht_probe_fp64_tflops.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
+    lib.sht_probe_fp64_tflops(ctypes.byref(fp64_dfma), ctypes.byref(fp64_dmma))
+    st = head["stages_ms"]
+    fft_bytes = (8 * I * J + 16 * (N + 1) * J) * nb           # per launch, per direction
+    leg_flops = 2 * J * (N + 1) * (N + 2) * nb                  # per launch, per direction (non-symmetric count)
+    cand = {
+        "k_fft (forward+inverse)": (st["syn"][0] + st["ana"][0], "hbm", 2 * fft_bytes, "GB/s"),
+        "k_leg (forward+inverse)": (st["syn"][1] + st["ana"][1], "tensor", 2 * leg_flops, "TFLOP/s"),
+    }
+    name = max(cand, key=lambda k: cand[k][0])
+    ms_k, bound, work, unit = cand[name]
+    if bound == "hbm":
+        achieved = work / (ms_k * 1e-3) / 1e9
+        peak = float(peaks.get("hbm_gbs", 6650.0))
+        pk_note = f"HBM copy bandwidth ({pk_kind})"
+    else:
+        achieved = work / (ms_k * 1e-3) / 1e12
+        if head_mode == "split":
+            peak = float(peaks.get("bf16_tflops", 1590.0))
+            pk_note = f"dense bf16 ({pk_kind})"
+        else:
+            peak = float(fp64_dmma.value)
+            pk_note = "FP64 mma.sync probe measured in this run"
+    roofline = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                "frac": achieved / peak if peak else None, "traffic": None, "peak_source": pk_note,
+                "stage_ms_per_step": {"synthesis[fft,legendre,spectral]": st["syn"],
+                                      "analysis[fft,legendre,spectral]": st["ana"]},
+                "fft_roofline_frac_of_hbm": (2 * fft_bytes / ((st["syn"][0] + st["ana"][0]) * 1e-3) / 1e9)
+                / float(peaks.get("hbm_gbs", 6650.0)),
+                "legendre_frac_of_fp64": (2 * leg_flops / ((st["syn"][1] + st["ana"][1]) * 1e-3) / 1e12)
+                / max(fp64_dmma.value, 1e-9)}
+
+    # e2e through the host-pointer C-ABI
+    e2e = None
+    if not args.no_e2e:
+        import torch as _t
+        wh = _t.empty((nb, L), dtype=_t.float64).pin_memory()
+        wh.copy_(w_in.cpu())
+        gh = _t.empty((nb, J, I), dtype=_t.float64).pin_memory()
+        wo = _t.empty((nb, L), dtype=_t.float64).pin_memory()
+        sht.set_precision(P.SHT_PREC_SPLIT if head_mode == "split" else P.SHT_PREC_FP64)
+        for _ in range(2):
+            lib.sht_xya_wa(h, VP(wh.data_ptr()), nb, VP(gh.data_ptr()))
+            lib.sht_wa_xya(h, VP(gh.data_ptr()), nb, VP(wo.data_ptr()))
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            s1 = lib.sht_xya_wa(h, VP(wh.data_ptr()), nb, VP(gh.data_ptr()))
+            s2 = lib.sht_wa_xya(h, VP(gh.data_ptr()), nb, VP(wo.data_ptr()))
+            if s1 or s2:
+                raise RuntimeError(lib.sht_last_error().decode())
+        el = max_over_ranks(time.perf_counter() - t0)
+        e2e = {"value": world * nb * args.steps / el, "unit": UNIT,
+               "h2d_bytes_per_step": 8 * nb * (L + I * J), "d2h_bytes_per_step": 8 * nb * (I * J + L),
+               "path": "sht_xya_wa + sht_wa_xya on pinned host arrays (synchronous C-ABI calls, host clock)",
+               "relerr": _rel(wo.numpy(), wh.numpy())}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(nb)
+
+    if rank == 0:
+        rec = {
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded spectra (n+1)^-2, seed 20261203)",
+            "config": {"workload": f"{GRID} L{LEVELS} x {FIELDS} fields round trip (xya_wa then wa_xya)",
+                       "field_levels_per_gpu": nb, "im": I, "jm": J, "nm": N,
+                       "precision": head_mode, "l2": "flushed (256 MiB write) between steps, outside the timed events",
+                       "parallelism": f"replicas x{world}"},
+            "precision_modes": {m: {k: v for k, v in r.items() if k != "clocks"} for m, r in results.items()},
+            "split_vs_fp64": (results["split"]["value"] / results["fp64"]["value"])
+            if "value" in results.get("split", {}) and "value" in results.get("fp64", {}) else None,
+            "relerr": head["relerr"],
+            "roofline": roofline,
+            "fp64_peak_tflops": {"dfma": fp64_dfma.value, "dmma": fp64_dmma.value},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": head["clocks"],
+            "gpu_launches": head["launches"],
+        }
+        print(json.dumps(rec))
+    sht.final()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

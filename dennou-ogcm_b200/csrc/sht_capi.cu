@@ -1,0 +1,588 @@
+// sht_capi.cu -- the extern "C" boundary (include/dogcm_sht.h).
+//
+// Each SpmlUtil_mod operator is composed from three device stages:
+//   analysis:  longitude FFT (row scale) -> Legendre contraction -> pack (+ recurrence)
+//   synthesis: unpack (+ recurrence) -> Legendre contraction -> longitude FFT (row scale)
+// Two-input operators (w_AlphaOptr_xy, calc_UVCosLat2VorDiv, xy_AlphaOptr_w,
+// calc_VorDiv2UV) run both inputs as one batch of 2 nb columns through a
+// single pass. The reference instead calls SPMODEL once per input and per
+// derivative (SpmlUtil_mod.f90:308-312, 335-338, 410, 426).
+#include "sht_internal.h"
+
+#include <atomic>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+namespace sht {
+
+static thread_local std::string g_last_error;
+static std::atomic<long long> g_launches{0};
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+int cuda_fail(cudaError_t e, const char *what)
+{
+  char buf[512];
+  snprintf(buf, sizeof(buf), "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+  g_last_error = buf;
+  if (e == cudaErrorMemoryAllocation) return SHT_ERR_ALLOC;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SHT_ERR_NO_DEVICE;
+  return SHT_ERR_CUDA;
+}
+void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+namespace {
+
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int dev)
+  {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) ok = (cudaSetDevice(dev) == cudaSuccess);
+  }
+  ~DeviceGuard()
+  {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+bool live(const sht_plan *p) { return p && p->magic == kPlanMagic; }
+
+int check_plan(const sht_plan *p)
+{
+  if (!live(p)) {
+    set_error("plan is not initialised");
+    return SHT_ERR_NOT_INITIALIZED;
+  }
+  return SHT_OK;
+}
+
+// Device workspace: Fourier array F, internal spectral S, spectral temp W.
+struct Workspace {
+  double2 *F;
+  double2 *S;
+  double *W;
+};
+
+int ensure_ws(sht_plan *p, int ncol, int nb_temp, Workspace *ws)
+{
+  const size_t fbytes = sizeof(double2) * (size_t)(p->N + 1) * ncol * p->J;
+  const size_t sbytes = sizeof(double2) * (size_t)p->R * ncol;
+  const size_t wbytes = sizeof(double) * (size_t)p->L * nb_temp;
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t need = al(fbytes) + al(sbytes) + al(wbytes);
+  if (need > p->ws_bytes) {
+    if (p->d_ws) {
+      cudaStreamSynchronize(p->stream);
+      cudaFree(p->d_ws);
+      p->d_ws = nullptr;
+      p->ws_bytes = 0;
+    }
+    cudaError_t e = cudaMalloc(&p->d_ws, need);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(workspace)");
+    p->ws_bytes = need;
+  }
+  char *base = static_cast<char *>(p->d_ws);
+  ws->F = reinterpret_cast<double2 *>(base);
+  ws->S = reinterpret_cast<double2 *>(base + al(fbytes));
+  ws->W = reinterpret_cast<double *>(base + al(fbytes) + al(sbytes));
+  return SHT_OK;
+}
+
+void mark(sht_plan *p, int k, cudaStream_t s)
+{
+  if (p->timing.on) cudaEventRecord(p->timing.ev[k], s);
+}
+
+int leg_fwd(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
+{
+  if (p->precision == SHT_PREC_SPLIT) return launch_leg_fwd_split(p, F, ncol, S, s);
+  return launch_leg_fwd_fp64(p, F, ncol, S, s);
+}
+int leg_inv(sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s)
+{
+  if (p->precision == SHT_PREC_SPLIT) return launch_leg_inv_split(p, S, ncol, F, s);
+  return launch_leg_inv_fp64(p, S, ncol, F, s);
+}
+
+// timing convention: ev[0] start, ev[1] after stage A, ev[2] after stage B, ev[3] end
+void finish_timing(sht_plan *p, bool analysis)
+{
+  if (!p->timing.on) return;
+  cudaEventSynchronize(p->timing.ev[3]);
+  float a = 0, b = 0, c = 0;
+  cudaEventElapsedTime(&a, p->timing.ev[0], p->timing.ev[1]);
+  cudaEventElapsedTime(&b, p->timing.ev[1], p->timing.ev[2]);
+  cudaEventElapsedTime(&c, p->timing.ev[2], p->timing.ev[3]);
+  if (analysis) { p->timing.ms_fft = a; p->timing.ms_leg = b; p->timing.ms_spec = c; }
+  else { p->timing.ms_spec = a; p->timing.ms_leg = b; p->timing.ms_fft = c; }
+}
+
+// grid inputs g0 (and g1) -> spectral outputs w0 (and w1)
+int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const double *g1, int nb,
+                 double *w0, double *w1)
+{
+  const int nin = g1 ? 2 : 1, ncol = nin * nb;
+  Workspace ws;
+  int rc = ensure_ws(p, ncol, 0, &ws);
+  if (rc) return rc;
+  cudaStream_t s = p->stream;
+  mark(p, 0, s);
+  if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s))) return rc;
+  mark(p, 1, s);
+  if ((rc = leg_fwd(p, ws.F, ncol, ws.S, s))) return rc;
+  mark(p, 2, s);
+  if ((rc = launch_pack(p, pack_op, ws.S, ncol, nb, w0, w1, s))) return rc;
+  mark(p, 3, s);
+  return SHT_OK;
+}
+
+// spectral inputs w0 (and w1) -> grid outputs g0 (and g1, for two-output ops)
+int run_synthesis(sht_plan *p, int unpack_op, int rs, const double *w0, const double *w1, int nb,
+                  double *g0, double *g1)
+{
+  const int nout = g1 ? 2 : 1, ncol = nout * nb;
+  Workspace ws;
+  int rc = ensure_ws(p, ncol, 0, &ws);
+  if (rc) return rc;
+  cudaStream_t s = p->stream;
+  mark(p, 0, s);
+  if ((rc = launch_unpack(p, unpack_op, w0, w1, nb, ws.S, ncol, s))) return rc;
+  mark(p, 1, s);
+  if ((rc = leg_inv(p, ws.S, ncol, ws.F, s))) return rc;
+  mark(p, 2, s);
+  if ((rc = launch_fft_inv(p, ws.F, ncol, 0, ncol, g0, g1, nb, rs, s))) return rc;
+  mark(p, 3, s);
+  return SHT_OK;
+}
+
+enum Op : int {
+  OP_W_XY, OP_XY_W, OP_DIVLAMBDA, OP_DIVMU, OP_GRADLAMBDA, OP_GRADMU, OP_GRADLON, OP_GRADLAT,
+  OP_W_ALPHA, OP_XY_ALPHA, OP_UV2VORDIV, OP_VORDIV2UV, OP_LAPLA, OP_LAPLAINV,
+  OP_AVRLONLAT, OP_INTLONLAT, OP_YA_AVRLON, OP_YA_INTLON
+};
+
+struct OpShape {
+  int nin, nout;
+  bool in_grid, out_grid;  // else spectral (reductions: out sized separately)
+};
+
+OpShape shape_of(int op)
+{
+  switch (op) {
+  case OP_W_XY: case OP_DIVLAMBDA: case OP_DIVMU: return {1, 1, true, false};
+  case OP_XY_W: case OP_GRADLAMBDA: case OP_GRADMU: case OP_GRADLON: case OP_GRADLAT: return {1, 1, false, true};
+  case OP_W_ALPHA: return {2, 1, true, false};
+  case OP_XY_ALPHA: return {2, 1, false, true};
+  case OP_UV2VORDIV: return {2, 2, true, false};
+  case OP_VORDIV2UV: return {2, 2, false, true};
+  case OP_LAPLA: case OP_LAPLAINV: return {1, 1, false, false};
+  default: return {1, 1, true, false};
+  }
+}
+
+// run an operator on device pointers (plan mutex held by the caller)
+int run_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1)
+{
+  if (nb == 0) return SHT_OK;
+  switch (op) {
+  case OP_W_XY: return run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, i0, nullptr, nb, o0, nullptr);
+  case OP_DIVLAMBDA: return run_analysis(p, PACK_DIVLAMBDA, RS_FWD_INV1MMU2, i0, nullptr, nb, o0, nullptr);
+  case OP_DIVMU: return run_analysis(p, PACK_DIVMU, RS_FWD_INV1MMU2, i0, nullptr, nb, o0, nullptr);
+  case OP_W_ALPHA: return run_analysis(p, PACK_ALPHA, RS_FWD_INV1MMU2, i0, i1, nb, o0, nullptr);
+  case OP_UV2VORDIV: return run_analysis(p, PACK_VORDIV, RS_FWD_INV1MMU2, i0, i1, nb, o0, o1);
+  case OP_XY_W: return run_synthesis(p, UNPACK_PLAIN, RS_INV_PLAIN, i0, nullptr, nb, o0, nullptr);
+  case OP_GRADLAMBDA: return run_synthesis(p, UNPACK_GRADLAMBDA, RS_INV_PLAIN, i0, nullptr, nb, o0, nullptr);
+  case OP_GRADMU: return run_synthesis(p, UNPACK_GRADMU, RS_INV_PLAIN, i0, nullptr, nb, o0, nullptr);
+  case OP_GRADLON: return run_synthesis(p, UNPACK_GRADLAMBDA, RS_INV_INVCOS, i0, nullptr, nb, o0, nullptr);
+  case OP_GRADLAT: return run_synthesis(p, UNPACK_GRADMU, RS_INV_INVCOS, i0, nullptr, nb, o0, nullptr);
+  case OP_XY_ALPHA: return run_synthesis(p, UNPACK_ALPHA, RS_INV_INVA1MMU2, i0, i1, nb, o0, nullptr);
+  case OP_VORDIV2UV: return run_synthesis(p, UNPACK_VORDIV2UV, RS_INV_INVACOS, i0, i1, nb, o0, o1);
+  case OP_LAPLA: return launch_lapla(p, i0, nb, o0, false, p->stream);
+  case OP_LAPLAINV: return launch_lapla(p, i0, nb, o0, true, p->stream);
+  case OP_INTLONLAT: return launch_lonlat_reduce(p, i0, nb, o0, 0, p->stream);
+  case OP_AVRLONLAT: return launch_lonlat_reduce(p, i0, nb, o0, 1, p->stream);
+  case OP_YA_INTLON: return launch_lonlat_reduce(p, i0, nb, o0, 2, p->stream);
+  case OP_YA_AVRLON: return launch_lonlat_reduce(p, i0, nb, o0, 3, p->stream);
+  default: set_error("unknown operator"); return SHT_ERR_INVALID_ARG;
+  }
+}
+
+size_t out_count(const sht_plan *p, int op, int nb)
+{
+  switch (op) {
+  case OP_AVRLONLAT: case OP_INTLONLAT: return (size_t)nb;
+  case OP_YA_AVRLON: case OP_YA_INTLON: return (size_t)nb * p->J;
+  default: return shape_of(op).out_grid ? (size_t)nb * p->I * p->J : (size_t)nb * p->L;
+  }
+}
+
+int check_args(const sht_plan *p, int op, const double *i0, const double *i1, int nb, const double *o0, const double *o1)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  const OpShape sh = shape_of(op);
+  if (nb < 0) { set_error("nb must be >= 0"); return SHT_ERR_INVALID_ARG; }
+  if (nb == 0) return SHT_OK;
+  if (!i0 || (sh.nin == 2 && !i1) || !o0 || (sh.nout == 2 && !o1)) {
+    set_error("null array argument");
+    return SHT_ERR_INVALID_ARG;
+  }
+  return SHT_OK;
+}
+
+// Device grid arrays are read and written as 16-byte pairs of doubles.
+int check_dev_alignment(int op, const double *i0, const double *i1, const double *o0, const double *o1)
+{
+  const OpShape sh = shape_of(op);
+  auto mis = [](const double *x) { return x && (reinterpret_cast<uintptr_t>(x) & 15u) != 0; };
+  if ((sh.in_grid && (mis(i0) || mis(i1))) || (sh.out_grid && (mis(o0) || mis(o1)))) {
+    set_error("device grid arrays must be 16-byte aligned");
+    return SHT_ERR_INVALID_ARG;
+  }
+  return SHT_OK;
+}
+
+int api_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1)
+{
+  int rc = check_args(p, op, i0, i1, nb, o0, o1);
+  if (rc || nb == 0) return rc;
+  if ((rc = check_dev_alignment(op, i0, i1, o0, o1))) return rc;
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
+  rc = run_dev(p, op, i0, i1, nb, o0, o1);
+  if (!rc) finish_timing(p, !shape_of(op).out_grid);
+  return rc;
+}
+
+int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1)
+{
+  int rc = check_args(p, op, i0, i1, nb, o0, o1);
+  if (rc || nb == 0) return rc;
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
+  const OpShape sh = shape_of(op);
+  const size_t nin_each = sh.in_grid ? (size_t)nb * p->I * p->J : (size_t)nb * p->L;
+  const size_t nout_each = out_count(p, op, nb);
+  // each staging buffer starts on a 256-byte boundary (the longitude transform
+  // moves grid rows as 16-byte pairs; lm = (nm+1)^2 may be odd)
+  auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };  // in doubles
+  const size_t need = sizeof(double) * (al(nin_each) * sh.nin + al(nout_each) * sh.nout) + 1024;
+  cudaError_t e;
+  if (need > p->io_bytes) {
+    if (p->d_io) { cudaStreamSynchronize(p->stream); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
+    if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
+    p->io_bytes = need;
+  }
+  double *d = static_cast<double *>(p->d_io);
+  double *di0 = d, *di1 = d + al(nin_each), *do0 = d + al(nin_each) * sh.nin, *do1 = do0 + al(nout_each);
+  cudaStream_t s = p->stream;
+  if ((e = cudaMemcpyAsync(di0, i0, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_fail(e, "H2D");
+  if (sh.nin == 2 && (e = cudaMemcpyAsync(di1, i1, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_fail(e, "H2D");
+  rc = run_dev(p, op, di0, sh.nin == 2 ? di1 : nullptr, nb, do0, sh.nout == 2 ? do1 : nullptr);
+  if (rc) return rc;
+  if ((e = cudaMemcpyAsync(o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "D2H");
+  if (sh.nout == 2 && (e = cudaMemcpyAsync(o1, do1, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "D2H");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
+  finish_timing(p, !sh.out_grid);
+  return SHT_OK;
+}
+
+void free_plan(sht_plan *p)
+{
+  cudaFree(p->d_mu); cudaFree(p->d_wgt); cudaFree(p->d_rowscale); cudaFree(p->d_P);
+  cudaFree(p->d_poff); cudaFree(p->d_rowoff); cudaFree(p->d_eps); cudaFree(p->d_tw);
+  cudaFree(p->d_twI); cudaFree(p->d_rn); cudaFree(p->d_spec_tiles);
+  cudaFree(p->d_ws); cudaFree(p->d_io);
+  free_split_tables(p);
+  for (auto &ev : p->timing.ev)
+    if (ev) cudaEventDestroy(ev);
+  if (p->own_stream) cudaStreamDestroy(p->own_stream);
+}
+
+}  // namespace
+}  // namespace sht
+
+using namespace sht;
+
+extern "C" {
+
+const char *sht_status_string(int status)
+{
+  switch (status) {
+  case SHT_OK: return "ok";
+  case SHT_ERR_INVALID_ARG: return "invalid argument";
+  case SHT_ERR_UNSUPPORTED_SIZE: return "unsupported grid size";
+  case SHT_ERR_NOT_INITIALIZED: return "plan not initialised";
+  case SHT_ERR_CUDA: return "CUDA error";
+  case SHT_ERR_NO_DEVICE: return "no CUDA device";
+  case SHT_ERR_ALLOC: return "allocation failed";
+  case SHT_ERR_DEVICE_TIMEOUT: return "device-side wait timed out";
+  case SHT_ERR_TOO_LARGE: return "request exceeds capacity";
+  default: return "unknown status";
+  }
+}
+
+const char *sht_last_error(void) { return g_last_error.c_str(); }
+
+int sht_l_nm(int n, int m) { return n * (n + 1) + m + 1; }
+
+int sht_nm_l(int l, int *n, int *m)
+{
+  if (l < 1 || !n || !m) { set_error("nm_l: bad argument"); return SHT_ERR_INVALID_ARG; }
+  int nn = (int)std::floor(std::sqrt((double)(l - 1)));
+  while ((nn + 1) * (nn + 1) <= l - 1) ++nn;
+  while (nn * nn > l - 1) --nn;
+  *n = nn;
+  *m = (l - 1) - nn * (nn + 1);
+  return SHT_OK;
+}
+
+int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
+{
+  if (!out) { set_error("init: plan pointer is NULL"); return SHT_ERR_INVALID_ARG; }
+  *out = nullptr;
+  if (nm == -1) nm = (im - 1) / 3;
+  int lg = 0;
+  while ((1 << lg) < im) ++lg;
+  if (im < 16 || im > 2048 || (1 << lg) != im) {
+    set_error("init: im must be a power of two in [16, 2048]");
+    return SHT_ERR_UNSUPPORTED_SIZE;
+  }
+  if (jm < 2 || (jm & 1)) { set_error("init: jm must be even and >= 2"); return SHT_ERR_UNSUPPORTED_SIZE; }
+  if (nm < 0 || im < 2 * nm + 2 || jm <= nm) {
+    set_error("init: need 0 <= nm, im >= 2 nm + 2 and jm > nm");
+    return SHT_ERR_UNSUPPORTED_SIZE;
+  }
+  if (nm > 1023 || !(radius > 0.0) || km < 0) { set_error("init: bad nm/radius/km"); return SHT_ERR_INVALID_ARG; }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    set_error(std::string("init: no CUDA device: ") + cudaGetErrorString(e));
+    return SHT_ERR_NO_DEVICE;
+  }
+  sht_plan *p = new (std::nothrow) sht_plan();
+  if (!p) { set_error("init: host allocation failed"); return SHT_ERR_ALLOC; }
+  p->I = im; p->J = jm; p->N = nm; p->K = km; p->JH = jm / 2; p->NC = im / 2; p->radius = radius;
+  cudaGetDevice(&p->device);
+  int rc = SHT_OK;
+  if ((e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking)) != cudaSuccess) rc = cuda_fail(e, "stream create");
+  p->stream = p->own_stream;
+  for (int k = 0; k < 8 && !rc; ++k)
+    if ((e = cudaEventCreate(&p->timing.ev[k])) != cudaSuccess) rc = cuda_fail(e, "event create");
+  if (!rc) rc = build_tables(p);
+  if (rc) {
+    free_plan(p);
+    delete p;
+    return rc;
+  }
+  p->magic = kPlanMagic;
+  *out = p;
+  return SHT_OK;
+}
+
+int sht_final(sht_plan *p)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  {
+    std::lock_guard<std::mutex> lk(p->mtx);
+    DeviceGuard g(p->device);
+    cudaStreamSynchronize(p->stream);
+    p->magic = 0;
+    free_plan(p);
+  }
+  delete p;
+  return SHT_OK;
+}
+
+int sht_is_initialized(const sht_plan *p) { return live(p) ? 1 : 0; }
+
+int sht_dims(const sht_plan *p, int *im, int *jm, int *nm, int *lm)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (im) *im = p->I;
+  if (jm) *jm = p->J;
+  if (nm) *nm = p->N;
+  if (lm) *lm = p->L;
+  return SHT_OK;
+}
+
+int sht_grid_info(const sht_plan *p, double *x_lon, double *y_lat, double *x_lon_weight, double *y_lat_weight)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  for (int i = 0; i < p->I; ++i) {
+    if (x_lon) x_lon[i] = 2.0 * M_PI * i / p->I;
+    if (x_lon_weight) x_lon_weight[i] = 2.0 * M_PI / p->I;
+  }
+  for (int j = 0; j < p->J; ++j) {
+    if (y_lat) y_lat[j] = std::asin(p->h_mu[j]);
+    if (y_lat_weight) y_lat_weight[j] = 2.0 * p->h_wgt[j];
+  }
+  return SHT_OK;
+}
+
+int sht_rn(const sht_plan *p, double *rn)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (!rn) { set_error("rn: NULL output"); return SHT_ERR_INVALID_ARG; }
+  for (int n = 0; n <= p->N; ++n)
+    for (int m = -n; m <= n; ++m) rn[n * (n + 1) + m] = -(double)n * (n + 1);
+  return SHT_OK;
+}
+
+int sht_set_precision(sht_plan *p, int mode)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (mode != SHT_PREC_FP64 && mode != SHT_PREC_SPLIT) { set_error("unknown precision mode"); return SHT_ERR_INVALID_ARG; }
+  std::lock_guard<std::mutex> lk(p->mtx);
+  p->precision = mode;
+  return SHT_OK;
+}
+
+int sht_get_precision(const sht_plan *p, int *mode)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (!mode) { set_error("NULL output"); return SHT_ERR_INVALID_ARG; }
+  *mode = p->precision;
+  return SHT_OK;
+}
+
+int sht_set_stream(sht_plan *p, void *stream)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(p->mtx);
+  p->stream = static_cast<cudaStream_t>(stream);
+  return SHT_OK;
+}
+
+int sht_synchronize(sht_plan *p)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  DeviceGuard g(p->device);
+  cudaError_t e = cudaStreamSynchronize(p->stream);
+  return e == cudaSuccess ? SHT_OK : cuda_fail(e, "synchronize");
+}
+
+int sht_set_timing(sht_plan *p, int on)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  p->timing.on = on != 0;
+  return SHT_OK;
+}
+
+int sht_last_timing(const sht_plan *p, float *ms_fft, float *ms_legendre, float *ms_spectral)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (ms_fft) *ms_fft = p->timing.ms_fft;
+  if (ms_legendre) *ms_legendre = p->timing.ms_leg;
+  if (ms_spectral) *ms_spectral = p->timing.ms_spec;
+  return SHT_OK;
+}
+
+long long sht_launch_count(void) { return g_launches.load(); }
+
+#define SHT_G2S(name, op)                                                                  \
+  int name(sht_plan *p, const double *x, int nb, double *w) { return api_host(p, op, x, nullptr, nb, w, nullptr); } \
+  int name##_dev(sht_plan *p, const double *x, int nb, double *w) { return api_dev(p, op, x, nullptr, nb, w, nullptr); }
+
+SHT_G2S(sht_wa_xya, OP_W_XY)
+SHT_G2S(sht_xya_wa, OP_XY_W)
+SHT_G2S(sht_wa_divlambda_xya, OP_DIVLAMBDA)
+SHT_G2S(sht_wa_divmu_xya, OP_DIVMU)
+SHT_G2S(sht_xya_gradlambda_wa, OP_GRADLAMBDA)
+SHT_G2S(sht_xya_gradmu_wa, OP_GRADMU)
+SHT_G2S(sht_xya_gradlon_wa, OP_GRADLON)
+SHT_G2S(sht_xya_gradlat_wa, OP_GRADLAT)
+SHT_G2S(sht_wa_lapla_wa, OP_LAPLA)
+SHT_G2S(sht_wa_laplainv_wa, OP_LAPLAINV)
+SHT_G2S(sht_avrlonlat_xya, OP_AVRLONLAT)
+SHT_G2S(sht_intlonlat_xya, OP_INTLONLAT)
+SHT_G2S(sht_ya_avrlon_xya, OP_YA_AVRLON)
+SHT_G2S(sht_ya_intlon_xya, OP_YA_INTLON)
+
+int sht_wa_alphaoptr_xya(sht_plan *p, const double *a, const double *b, int nb, double *w)
+{ return api_host(p, OP_W_ALPHA, a, b, nb, w, nullptr); }
+int sht_wa_alphaoptr_xya_dev(sht_plan *p, const double *a, const double *b, int nb, double *w)
+{ return api_dev(p, OP_W_ALPHA, a, b, nb, w, nullptr); }
+int sht_xya_alphaoptr_wa(sht_plan *p, const double *a, const double *b, int nb, double *x)
+{ return api_host(p, OP_XY_ALPHA, a, b, nb, x, nullptr); }
+int sht_xya_alphaoptr_wa_dev(sht_plan *p, const double *a, const double *b, int nb, double *x)
+{ return api_dev(p, OP_XY_ALPHA, a, b, nb, x, nullptr); }
+int sht_uvcoslat2vordiv(sht_plan *p, const double *u, const double *v, int nb, double *vor, double *div)
+{ return api_host(p, OP_UV2VORDIV, u, v, nb, vor, div); }
+int sht_uvcoslat2vordiv_dev(sht_plan *p, const double *u, const double *v, int nb, double *vor, double *div)
+{ return api_dev(p, OP_UV2VORDIV, u, v, nb, vor, div); }
+int sht_vordiv2uv(sht_plan *p, const double *vor, const double *div, int nb, double *u, double *v)
+{ return api_host(p, OP_VORDIV2UV, vor, div, nb, u, v); }
+int sht_vordiv2uv_dev(sht_plan *p, const double *vor, const double *div, int nb, double *u, double *v)
+{ return api_dev(p, OP_VORDIV2UV, vor, div, nb, u, v); }
+
+static int diffuse_impl(sht_plan *p, double *w, int nb, const double *coef, double dt, const double *filter, bool host)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (nb < 0 || (nb > 0 && (!w || !coef))) { set_error("diffuse: bad argument"); return SHT_ERR_INVALID_ARG; }
+  if (nb == 0) return SHT_OK;
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard g(p->device);
+  cudaStream_t s = p->stream;
+  cudaError_t e;
+  if (!host) return launch_diffuse(p, w, nb, coef, dt, filter, s);
+  const size_t nw = (size_t)nb * p->L, need = sizeof(double) * (nw + 2 * p->L) + 1024;
+  if (need > p->io_bytes) {
+    if (p->d_io) { cudaStreamSynchronize(s); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
+    if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
+    p->io_bytes = need;
+  }
+  double *dw = static_cast<double *>(p->d_io), *dc = dw + nw, *df = dc + p->L;
+  if ((e = cudaMemcpyAsync(dw, w, sizeof(double) * nw, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dc, coef, sizeof(double) * p->L, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (filter && (e = cudaMemcpyAsync(df, filter, sizeof(double) * p->L, cudaMemcpyHostToDevice, s)) != cudaSuccess))
+    return cuda_fail(e, "H2D");
+  if ((rc = launch_diffuse(p, dw, nb, dc, dt, filter ? df : nullptr, s))) return rc;
+  if ((e = cudaMemcpyAsync(w, dw, sizeof(double) * nw, cudaMemcpyDeviceToHost, s)) != cudaSuccess) return cuda_fail(e, "D2H");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "diffuse");
+  return SHT_OK;
+}
+
+int sht_wa_diffuse(sht_plan *p, double *w, int nb, const double *coef, double dt, const double *filter)
+{ return diffuse_impl(p, w, nb, coef, dt, filter, true); }
+int sht_wa_diffuse_dev(sht_plan *p, double *w, int nb, const double *coef, double dt, const double *filter)
+{ return diffuse_impl(p, w, nb, coef, dt, filter, false); }
+
+int sht_roundtrip_diffuse_dev(sht_plan *p, double *xya, int nb, const double *coef, double dt, const double *filter)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (nb < 0 || (nb > 0 && !xya)) { set_error("roundtrip: bad argument"); return SHT_ERR_INVALID_ARG; }
+  if ((reinterpret_cast<uintptr_t>(xya) & 15u) != 0) { set_error("device grid arrays must be 16-byte aligned"); return SHT_ERR_INVALID_ARG; }
+  if (nb == 0) return SHT_OK;
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard g(p->device);
+  Workspace ws;
+  if ((rc = ensure_ws(p, nb, nb, &ws))) return rc;
+  if ((rc = run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, xya, nullptr, nb, ws.W, nullptr))) return rc;
+  if (coef && (rc = launch_diffuse(p, ws.W, nb, coef, dt, filter, p->stream))) return rc;
+  return run_synthesis(p, UNPACK_PLAIN, RS_INV_PLAIN, ws.W, nullptr, nb, xya, nullptr);
+}
+
+}  // extern "C"

@@ -1,0 +1,148 @@
+// sht_internal.h -- plan state, device layouts and kernel launchers of the
+// B200 spherical-harmonic transform.
+//
+// Device data layouts (all FP64):
+//   grid      xya[b][j][i]        b < nb field-levels, j < J (mu ascending), i < I
+//   spectral  wa[b][l]            SPML order l = n(n+1)+m, m in [-n, n]
+//   Fourier   F[m][col][j]        complex G^m(mu_j) for m <= N, col < ncol
+//                                 (ncol = nb, or 2 nb for two-input operators)
+//   internal  S[row][col]         complex coefficient of Pbar_n^m, row = rowoff(m) + n - m,
+//                                 n = m..N+1 (one extra degree so that the
+//                                 (1-mu^2) d/dmu recurrences close), rowoff(m) =
+//                                 sum_{m'<m} (N+2-m').
+//   Legendre  P[poff(m) + (n-m) JH + jh]  Pbar_n^m at the northern Gauss rows
+//                                 j = JH + jh (JH = J/2), n = m..N+1.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstddef>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/dogcm_sht.h"
+
+namespace sht {
+
+// Row-scale tables used by the longitude transforms (per Gauss row j).
+enum RowScale : int {
+  RS_FWD_PLAIN = 0,     // analysis: w_j / I
+  RS_FWD_INV1MMU2 = 1,  // analysis: w_j / (I (1 - mu_j^2))
+  RS_INV_PLAIN = 2,     // synthesis: 1
+  RS_INV_INVCOS = 3,    // synthesis: 1 / cos(phi_j)
+  RS_INV_INVA1MMU2 = 4, // synthesis: 1 / (a (1 - mu_j^2))
+  RS_INV_INVACOS = 5,   // synthesis: 1 / (a cos(phi_j))
+  RS_COUNT = 6
+};
+
+// Spectral-side operators applied between the SPML layout and the internal one.
+enum PackOp : int {
+  PACK_PLAIN = 0,      // w = c
+  PACK_DIVLAMBDA = 1,  // w = i m c
+  PACK_DIVMU = 2,      // w = D(c) = -((n+1) eps_n c_{n-1} - n eps_{n+1} c_{n+1})
+  PACK_ALPHA = 3,      // w = (i m cA + D(cB)) / a, D = the divmu form    (two column sets)
+  PACK_VORDIV = 4,     // vor = (i m cV - D(cU))/a, div = (i m cU + D(cV))/a
+};
+enum UnpackOp : int {
+  UNPACK_PLAIN = 0,      // a
+  UNPACK_GRADLAMBDA = 1, // i m a
+  UNPACK_GRADMU = 2,     // (k+2) eps_{k+1} a_{k+1} - (k-1) eps_k a_{k-1}
+  UNPACK_ALPHA = 3,      // i m aA + GRADMU(aB)                   (two inputs)
+  UNPACK_VORDIV2UV = 4,  // psi, chi = -a^2 a/(n(n+1)); U = i m chi - GRADMU(psi), V = i m psi + GRADMU(chi)
+};
+
+struct Timing {
+  bool on = false;
+  cudaEvent_t ev[8] = {};
+  float ms_fft = 0.f, ms_leg = 0.f, ms_spec = 0.f;
+};
+
+}  // namespace sht
+
+struct sht_plan_s {
+  uint32_t magic = 0;
+  int I = 0, J = 0, N = 0, K = 0, JH = 0, NC = 0, L = 0;
+  int fa = 0, fb = 0;           // four-step split NC = 2^fa * 2^fb
+  long long R = 0;              // internal rows (N+1)(N+4)/2
+  double radius = 1.0;
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream used by all work of the plan
+  cudaStream_t own_stream = nullptr;  // stream created by sht_init (destroyed by sht_final)
+  int precision = SHT_PREC_FP64;
+
+  // device tables
+  double *d_mu = nullptr, *d_wgt = nullptr, *d_rowscale = nullptr;
+  double *d_P = nullptr;
+  long long *d_poff = nullptr;
+  int *d_rowoff = nullptr;
+  double *d_eps = nullptr;  // [m][n], n = 0..N+2
+  double2 *d_tw = nullptr;  // exp(-2 pi i k / NC), k < NC
+  double2 *d_twI = nullptr; // exp(-2 pi i k / I),  k < NC
+  double *d_rn = nullptr;   // -n(n+1) per l
+  int2 *d_spec_tiles = nullptr;  // (n, m0) tiles of the spectral conversions
+  int n_spec_tiles = 0;          // n = 0..N+1
+  int n_pack_tiles = 0;          // n = 0..N (a prefix of the list)
+
+  // host copies
+  std::vector<double> h_mu, h_wgt;
+  std::vector<int> h_rowoff;
+
+  // device workspace (Fourier + internal spectral), grown on demand
+  void *d_ws = nullptr;
+  size_t ws_bytes = 0;
+  // device staging for the host-pointer API, grown on demand
+  void *d_io = nullptr;
+  size_t io_bytes = 0;
+
+  // split-precision tables (built lazily)
+  void *tc_tables = nullptr;
+
+  std::mutex mtx;
+  sht::Timing timing;
+};
+
+namespace sht {
+
+constexpr uint32_t kPlanMagic = 0x53485442u;  // "SHTB"
+
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+void count_launch(int n = 1);
+
+// --- setup kernels (sht_setup.cu)
+int build_tables(sht_plan *p);
+
+// --- longitude transforms (sht_fft.cu)
+// grid (up to two source arrays: columns [0, nsplit) from g0, the rest from g1)
+// -> F[m][colF0 + col][j], scaled per row by rowscale table `rs`.
+int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
+                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s);
+// F -> grid (two destinations split at nsplit), scaled per row by `rs`.
+int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, int ncol,
+                   double *g0, double *g1, int nsplit, int rs, cudaStream_t s);
+
+// --- Legendre contraction, FP64 (sht_legendre.cu)
+int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
+int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
+
+// --- Legendre contraction, split precision on tcgen05 (sht_legendre_tc.cu)
+int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
+int launch_leg_inv_split(sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
+void free_split_tables(sht_plan *p);
+
+// --- spectral-side kernels (sht_spectral.cu)
+// internal S (ncolS columns; set A at col 0, set B at col nb) -> SPML wa outputs
+int launch_pack(const sht_plan *p, int op, const double2 *S, int ncolS, int nb, double *w0,
+                double *w1, cudaStream_t s);
+// SPML inputs -> internal S (ncolS columns)
+int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1, int nb,
+                  double2 *S, int ncolS, cudaStream_t s);
+int launch_lapla(const sht_plan *p, const double *w, int nb, double *out, bool inverse,
+                 cudaStream_t s);
+int launch_diffuse(const sht_plan *p, double *w, int nb, const double *coef, double dt,
+                   const double *filter, cudaStream_t s);
+int launch_lonlat_reduce(const sht_plan *p, const double *g, int nb, double *out, int kind,
+                         cudaStream_t s);
+
+}  // namespace sht

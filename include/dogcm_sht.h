@@ -1,0 +1,233 @@
+/*
+ * dogcm_sht.h -- C-ABI of the B200 spherical-harmonic transform library
+ * (libdogcm_sht.so).
+ *
+ * It replaces the horizontal part of dogcm's spectral utility module
+ * model/dogcm/src/util/math/SpmlUtil_mod.f90 (and the SPMODEL wa_module
+ * routines that module re-exports at SpmlUtil_mod.f90:105-135).  Every entry
+ * point cites the reference routine it stands in for.  A Fortran host binds
+ * these through ISO_C_BINDING.
+ *
+ * Conventions
+ *  - All arrays are FP64 and use the reference's Fortran layouts:
+ *      grid      xya(0:im-1, 1:jm, nb)  lon fastest, Gauss latitudes
+ *                ascending from the south pole;
+ *      spectral  wa(lm, nb), lm = (nm+1)^2, l_nm(n,m) = n(n+1)+m+1 (1-based).
+ *                wa(l_nm(n,0)) = a_n^0.  For m > 0, wa(l_nm(n,m)) = sqrt2 Re a_n^m
+ *                and wa(l_nm(n,-m)) = sqrt2 Im a_n^m, for the field
+ *                sum_n sum_m a_n^m Pbar_n^|m|(mu) e^{i m lambda}, where
+ *                int_{-1}^{1} Pbar^2 dmu = 2.
+ *    nb is the number of field-levels (the trailing dimension).  nb = 1 is the
+ *    single-level form (w_xy, xy_w, ...), nb = km the wa_/xya_ form.
+ *  - Every function returns an int status (SHT_OK = 0).  The reference
+ *    aborts through MessageNotify('E', ...) on misuse.  Here the caller maps a
+ *    nonzero status to that abort, and sht_last_error() gives the message.
+ *  - Functions without a suffix take HOST pointers and return when the
+ *    results are in host memory.  The *_dev variants take DEVICE pointers and
+ *    are ordered on the plan's stream (sht_set_stream).  They return once the
+ *    work is enqueued.
+ *  - Calls on one plan are serialised internally: the plan owns its device
+ *    workspace.  Different plans may be used from different host threads.
+ *  - There is no CPU fallback.  Without a usable CUDA device every compute
+ *    entry point returns SHT_ERR_CUDA or SHT_ERR_NO_DEVICE.
+ */
+#ifndef DOGCM_SHT_H
+#define DOGCM_SHT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SHT_API __attribute__((visibility("default")))
+#else
+#define SHT_API
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define SHT_OK                   0
+#define SHT_ERR_INVALID_ARG      1  /* null pointer, nb < 0, bad mode            */
+#define SHT_ERR_UNSUPPORTED_SIZE 2  /* grid the kernels do not cover (see sht_init) */
+#define SHT_ERR_NOT_INITIALIZED  3  /* plan is NULL or already finalised         */
+#define SHT_ERR_CUDA             4  /* a CUDA runtime call failed                */
+#define SHT_ERR_NO_DEVICE        5  /* no CUDA device visible                    */
+#define SHT_ERR_ALLOC            6  /* device or host allocation failed          */
+#define SHT_ERR_DEVICE_TIMEOUT   7  /* a bounded device-side wait ran out        */
+#define SHT_ERR_TOO_LARGE        8  /* request exceeds a fixed capacity          */
+
+/* precision modes of the Legendre contraction */
+#define SHT_PREC_FP64  0  /* plain FP64 on CUDA cores                             */
+#define SHT_PREC_SPLIT 1  /* FP64 operands sliced into low-precision integer
+                             pieces, exact tensor-core products, FP64 recombine  */
+
+typedef struct sht_plan_s sht_plan;
+
+/* Status text of a code, and the message of the last failure on this thread. */
+SHT_API const char *sht_status_string(int status);
+SHT_API const char *sht_last_error(void);
+
+/* ------------------------------------------------------------- plan/admin */
+
+/* SpmlUtil_Init(iMax, jMax, kMax, nMax, tMax, RPlanet, np)
+ * (SpmlUtil_mod.f90:192-241; wa_Initial at :218-223).
+ * im: longitudes (a power of two, 8..2048), jm: Gauss latitudes (even),
+ * km: levels (the default batch; informational), nm: triangular truncation
+ * (nm = -1 selects (im-1)/3 as in util/grid/DOGCM_GaussSpmVFvmGrid_mod.f90:209),
+ * radius: planetary radius (Radius in SpmlUtil_mod).  Requires
+ * im >= 2 nm + 2 and jm > nm.  Builds the Gauss nodes and weights and the
+ * associated-Legendre table on the device in FP64. */
+SHT_API int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **plan);
+
+/* SpmlUtil_Final (SpmlUtil_mod.f90:243-256).  Frees the plan. */
+SHT_API int sht_final(sht_plan *plan);
+
+/* isInitialzed (SpmlUtil_mod.f90:262-267). 1 if the plan is live. */
+SHT_API int sht_is_initialized(const sht_plan *plan);
+
+/* Grid sizes: im, jm, nm and lm = (nm+1)^2.  Any pointer may be NULL. */
+SHT_API int sht_dims(const sht_plan *plan, int *im, int *jm, int *nm, int *lm);
+
+/* get_SpmlGridInfo (SpmlUtil_mod.f90:271-295): x_Lon (im), y_Lat (jm, radians),
+ * x_Lon_Weight (im, sums to 2 pi), y_Lat_Weight (jm, sums to 2).
+ * Any output may be NULL. */
+SHT_API int sht_grid_info(const sht_plan *plan, double *x_lon, double *y_lat,
+                  double *x_lon_weight, double *y_lat_weight);
+
+/* l_nm / nm_l (re-exported at SpmlUtil_mod.f90:120): 1-based spectral index. */
+SHT_API int sht_l_nm(int n, int m);
+SHT_API int sht_nm_l(int l, int *n, int *m);
+
+/* rn(:,1) (SpmlUtil_mod.f90:135): Laplacian eigenvalue -n(n+1) per l. */
+SHT_API int sht_rn(const sht_plan *plan, double *rn);
+
+/* Precision of the Legendre contraction for the following calls
+ * (SHT_PREC_FP64 is the default). */
+SHT_API int sht_set_precision(sht_plan *plan, int mode);
+SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
+
+/* Stream for the *_dev calls (a cudaStream_t passed as void*; NULL = legacy
+ * default stream), and a wait for all work on it. */
+SHT_API int sht_set_stream(sht_plan *plan, void *stream);
+SHT_API int sht_synchronize(sht_plan *plan);
+
+/* ------------------------------------------------- transforms, host arrays */
+
+/* w_xy / wa_xya / wz_xyz: grid -> spectral analysis
+ * (SPMODEL wa_module via SpmlUtil_mod.f90:110; wz_xyz alias at
+ * model/old/sogcm/util/SpmlUtil_mod.f90:323-333). */
+SHT_API int sht_wa_xya(sht_plan *plan, const double *xya, int nb, double *wa);
+
+/* xy_w / xya_wa / xyz_wz: spectral -> grid synthesis (SpmlUtil_mod.f90:110;
+ * model/old/sogcm/util/SpmlUtil_mod.f90:308-320). */
+SHT_API int sht_xya_wa(sht_plan *plan, const double *wa, int nb, double *xya);
+
+/* w_DivLambda_xy: spectral of (1/(1-mu^2)) dA/dlambda (SpmlUtil_mod.f90:116). */
+SHT_API int sht_wa_divlambda_xya(sht_plan *plan, const double *xya, int nb, double *wa);
+
+/* w_DivMu_xy: spectral of dB/dmu (SpmlUtil_mod.f90:116). */
+SHT_API int sht_wa_divmu_xya(sht_plan *plan, const double *xya, int nb, double *wa);
+
+/* xy_GradLambda_w (d/dlambda), xy_GradMu_w ((1-mu^2) d/dmu),
+ * xy_GradLon_w ((1/cos phi) d/dlambda), xy_GradLat_w (d/dphi)
+ * (SpmlUtil_mod.f90:114-115). */
+SHT_API int sht_xya_gradlambda_wa(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_xya_gradmu_wa(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_xya_gradlon_wa(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_xya_gradlat_wa(sht_plan *plan, const double *wa, int nb, double *xya);
+
+/* w_AlphaOptr_xy / wa_AlphaOptr_xya: (DivLambda(A) + DivMu(B)) / a
+ * (SpmlUtil_mod.f90:398-412, 453-473). */
+SHT_API int sht_wa_alphaoptr_xya(sht_plan *plan, const double *xya_a, const double *xya_b,
+                         int nb, double *wa);
+
+/* xy_AlphaOptr_w / xya_AlphaOptr_wa: (GradLambda(A) + GradMu(B)) / (a cos^2 phi)
+ * (SpmlUtil_mod.f90:414-451). */
+SHT_API int sht_xya_alphaoptr_wa(sht_plan *plan, const double *wa_a, const double *wa_b,
+                         int nb, double *xya);
+
+/* calc_UVCosLat2VorDiv: Vor = H(V cos, -U cos), Div = H(U cos, V cos)
+ * (SpmlUtil_mod.f90:299-314, 342-368). Inputs are U cos phi and V cos phi. */
+SHT_API int sht_uvcoslat2vordiv(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
+                        int nb, double *wa_vor, double *wa_div);
+
+/* calc_VorDiv2UV: psi = a^2 LaplaInv(Vor), chi = a^2 LaplaInv(Div),
+ * U = cos * AlphaOptr(chi, -psi), V = cos * AlphaOptr(psi, chi)
+ * (SpmlUtil_mod.f90:316-340, 370-396). */
+SHT_API int sht_vordiv2uv(sht_plan *plan, const double *wa_vor, const double *wa_div,
+                  int nb, double *xya_u, double *xya_v);
+
+/* w_Lapla_w, w_LaplaInv_w (SpmlUtil_mod.f90:117): -n(n+1) w and its inverse
+ * with the n = 0 mode set to zero (HBEBarot_hspm_vfvm_mod.f90:295-298). */
+SHT_API int sht_wa_lapla_wa(sht_plan *plan, const double *wa, int nb, double *out);
+SHT_API int sht_wa_laplainv_wa(sht_plan *plan, const double *wa, int nb, double *out);
+
+/* Spectral backward-Euler lateral diffusion, in place:
+ * wa(l,k) <- filter(l) wa(l,k) / (1 - dt coef(l))
+ * (physics/DOGCM_Phys_hspm_vfvm_mod.f90:638-641, 741-742).  filter may be NULL
+ * (all ones).  coef and filter have lm entries. */
+SHT_API int sht_wa_diffuse(sht_plan *plan, double *wa, int nb, const double *coef, double dt,
+                   const double *filter);
+
+/* AvrLonLat_xy / IntLonLat_xy (SpmlUtil_mod.f90:123-124): one value per level;
+ * ya_AvrLon_xya / ya_IntLon_xya: out(jm, nb). */
+SHT_API int sht_avrlonlat_xya(sht_plan *plan, const double *xya, int nb, double *out);
+SHT_API int sht_intlonlat_xya(sht_plan *plan, const double *xya, int nb, double *out);
+SHT_API int sht_ya_avrlon_xya(sht_plan *plan, const double *xya, int nb, double *out);
+SHT_API int sht_ya_intlon_xya(sht_plan *plan, const double *xya, int nb, double *out);
+
+/* ------------------------------------------- transforms, device arrays */
+/* Same operations on device pointers, enqueued on the plan's stream. */
+SHT_API int sht_wa_xya_dev(sht_plan *plan, const double *xya, int nb, double *wa);
+SHT_API int sht_xya_wa_dev(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_wa_divlambda_xya_dev(sht_plan *plan, const double *xya, int nb, double *wa);
+SHT_API int sht_wa_divmu_xya_dev(sht_plan *plan, const double *xya, int nb, double *wa);
+SHT_API int sht_xya_gradlambda_wa_dev(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_xya_gradmu_wa_dev(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_xya_gradlon_wa_dev(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_xya_gradlat_wa_dev(sht_plan *plan, const double *wa, int nb, double *xya);
+SHT_API int sht_wa_alphaoptr_xya_dev(sht_plan *plan, const double *xya_a, const double *xya_b,
+                             int nb, double *wa);
+SHT_API int sht_xya_alphaoptr_wa_dev(sht_plan *plan, const double *wa_a, const double *wa_b,
+                             int nb, double *xya);
+SHT_API int sht_uvcoslat2vordiv_dev(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
+                            int nb, double *wa_vor, double *wa_div);
+SHT_API int sht_vordiv2uv_dev(sht_plan *plan, const double *wa_vor, const double *wa_div,
+                      int nb, double *xya_u, double *xya_v);
+SHT_API int sht_wa_lapla_wa_dev(sht_plan *plan, const double *wa, int nb, double *out);
+SHT_API int sht_wa_laplainv_wa_dev(sht_plan *plan, const double *wa, int nb, double *out);
+SHT_API int sht_wa_diffuse_dev(sht_plan *plan, double *wa, int nb, const double *coef, double dt,
+                       const double *filter);
+SHT_API int sht_avrlonlat_xya_dev(sht_plan *plan, const double *xya, int nb, double *out);
+SHT_API int sht_intlonlat_xya_dev(sht_plan *plan, const double *xya, int nb, double *out);
+SHT_API int sht_ya_avrlon_xya_dev(sht_plan *plan, const double *xya, int nb, double *out);
+SHT_API int sht_ya_intlon_xya_dev(sht_plan *plan, const double *xya, int nb, double *out);
+
+/* Fused round trip used by the implicit diffusion step
+ * (physics/DOGCM_Phys_hspm_vfvm_mod.f90:638-641):
+ * xya <- xy_w( filter * w_xy(xya) / (1 - dt coef) ), in place on device
+ * arrays.  coef/filter (lm entries, device pointers) may be NULL (plain
+ * round trip). */
+SHT_API int sht_roundtrip_diffuse_dev(sht_plan *plan, double *xya, int nb, const double *coef,
+                              double dt, const double *filter);
+
+/* ------------------------------------------------------------ diagnostics */
+
+/* Device time in milliseconds of the kernels of the last *_dev call, summed
+ * per stage (fft, legendre, spectral); NULL entries are skipped.  Timing is
+ * recorded only when enabled with sht_set_timing(plan, 1). */
+SHT_API int sht_set_timing(sht_plan *plan, int on);
+SHT_API int sht_last_timing(const sht_plan *plan, float *ms_fft, float *ms_legendre,
+                    float *ms_spectral);
+
+/* Number of kernel launches issued by this library since process start. */
+SHT_API long long sht_launch_count(void);
+
+/* FP64 throughput of the current device in TFLOP/s, measured by two
+ * dependency-free loops (DFMA, and mma.sync.m8n8k4.f64); the roofline
+ * denominator of the FP64 Legendre contraction.  Either pointer may be NULL. */
+SHT_API int sht_probe_fp64_tflops(double *tflops_dfma, double *tflops_dmma);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DOGCM_SHT_H */

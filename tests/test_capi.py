@@ -1,0 +1,70 @@
+"""C-ABI library: it loads, exports every symbol include/dogcm_sht.h declares, and
+its host-side logic (argument checks, index maps, status text) behaves without
+a GPU.  No compute call runs here."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from conftest import ROOT, pkg
+
+HEADER = os.path.join(ROOT, "include", "dogcm_sht.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"^SHT_API [^;]*?\b(sht_[a-z0-9_]+)\s*\(", txt, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert len(syms) >= 50
+    for s in ("sht_init", "sht_final", "sht_wa_xya", "sht_xya_wa", "sht_vordiv2uv", "sht_uvcoslat2vordiv"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol():
+    lib = pkg().load_library()
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_index_maps_and_status_text():
+    p = pkg()
+    assert p.l_nm(0, 0) == 1
+    for l in range(1, 2000):
+        n, m = p.nm_l(l)
+        assert p.l_nm(n, m) == l
+    lib = p.load_library()
+    assert lib.sht_status_string(0) == b"ok"
+    assert lib.sht_status_string(2) == b"unsupported grid size"
+
+
+@pytest.mark.parametrize("args", [(63, 32, 1, 21), (64, 31, 1, 21), (64, 32, 1, 40), (4096, 512, 1, 100),
+                                  (64, 16, 1, 21)])
+def test_init_rejects_unsupported_grids(args):
+    """Sizes are validated on the host before any device work (status 2)."""
+    lib = pkg().load_library()
+    h = ctypes.c_void_p()
+    st = lib.sht_init(*args, ctypes.c_double(1.0), ctypes.byref(h))
+    assert st == 2
+    assert not h.value
+
+
+def test_calls_on_null_plan_fail_cleanly():
+    lib = pkg().load_library()
+    buf = (ctypes.c_double * 8)()
+    assert lib.sht_wa_xya(None, buf, 1, buf) == 3
+    assert lib.sht_final(None) == 3
+    assert lib.sht_is_initialized(None) == 0
+    assert b"not initialised" in lib.sht_last_error()
+
+
+def test_init_without_device_reports_no_device(cuda_available):
+    if cuda_available:
+        pytest.skip("a CUDA device is present")
+    lib = pkg().load_library()
+    h = ctypes.c_void_p()
+    st = lib.sht_init(64, 32, 1, 21, ctypes.c_double(1.0), ctypes.byref(h))
+    assert st == 5

@@ -1,0 +1,229 @@
+"""GPU parity: every SpmlUtil operator through the C-ABI against the CPU oracle
+and the golden vectors.
+
+Tolerance: the plain FP64 path must match within 1e-11 per-field normwise
+relative error (max|gpu - ref| / max|ref| per field-level), the bound the
+transform is specified to.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import load_golden, pkg, relerr, workloads
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+GRIDS = [(32, 16, 10), (64, 32, 21), (128, 64, 42), (256, 128, 85), (512, 256, 170)]
+
+
+@pytest.fixture(scope="module")
+def plans():
+    cache = {}
+
+    def get(I, J, N, a=1.0):
+        key = (I, J, N, a)
+        if key not in cache:
+            cache[key] = (pkg().SpmlUtil(I, J, 1, N, None, a), O.OraclePlan(I, J, N, a))
+        return cache[key]
+
+    yield get
+    for g, _ in cache.values():
+        g.final()
+
+
+def _inputs(I, J, N, nb, seed=11, a=1.0):
+    rng = np.random.default_rng(seed)
+    W = workloads()
+    w = W.seeded_spectra(N, nb, 1.5, rng=rng)
+    w2 = W.seeded_spectra(N, nb, 2.0, rng=rng)
+    grid = rng.standard_normal((nb, J, I))
+    return w, w2, grid
+
+
+@pytest.mark.parametrize("tag", ["T21", "T10"])
+def test_golden(tag, plans):
+    g = load_golden(tag)
+    gpu, _ = plans(int(g["I"]), int(g["J"]), int(g["N"]), float(g["radius"]))
+    cs = np.cos(np.arcsin(g["mu"]))[None, :, None]
+    res = {
+        "xy_w": relerr(gpu.xya_wa(g["w"]), g["xy_w"]),
+        "w_xy_rand": relerr(gpu.wa_xya(g["grid_rand"]), g["w_xy_rand"]),
+        "gradlambda": relerr(gpu.xya_GradLambda_wa(g["w"]), g["gradlambda"]),
+        "gradmu": relerr(gpu.xya_GradMu_wa(g["w"]), g["gradmu"]),
+        "gradlon": relerr(gpu.xya_GradLon_wa(g["w"]), g["gradlon"]),
+        "gradlat": relerr(gpu.xya_GradLat_wa(g["w"]), g["gradlat"]),
+        "divlambda": relerr(gpu.wa_DivLambda_xya(g["divA"]), g["divlambda"]),
+        "divmu": relerr(gpu.wa_DivMu_xya(g["divB"]), g["divmu"]),
+        "w_alpha": relerr(gpu.wa_AlphaOptr_xya(g["divA"], g["divB"]), g["w_alpha"]),
+        "xy_alpha": relerr(gpu.xya_AlphaOptr_wa(g["w"], g["w2"]), g["xy_alpha"]),
+        "avr": relerr(gpu.AvrLonLat_xy(g["xy_w"]), g["avr"]),
+    }
+    u, v = gpu.calc_VorDiv2UV(g["w"], g["w2"])
+    res["U"], res["V"] = relerr(u, g["U"]), relerr(v, g["V"])
+    vo, di = gpu.calc_UVCosLat2VorDiv(g["U"] * cs, g["V"] * cs)
+    res["vor"], res["div"] = relerr(vo, g["vor"]), relerr(di, g["div"])
+    bad = {k: v for k, v in res.items() if v > TOL}
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_analysis_synthesis_vs_oracle(grid, plans):
+    I, J, N = grid
+    gpu, ora = plans(I, J, N)
+    w, w2, x = _inputs(I, J, N, 5)
+    assert relerr(gpu.xya_wa(w), ora.xya_wa(w)) < TOL
+    assert relerr(gpu.wa_xya(x), ora.wa_xya(x)) < TOL
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_derivatives_vs_oracle(grid, plans):
+    I, J, N = grid
+    a = 6.371e6
+    gpu, ora = plans(I, J, N, a)
+    w, w2, x = _inputs(I, J, N, 4, seed=12)
+    cs2 = np.cos(gpu.y_Lat)[None, :, None] ** 2
+    A, B = ora.xya_wa(w) * cs2, ora.xya_wa(w2) * cs2  # U cos phi-like, vanish at the poles
+    res = {
+        "gradlambda": relerr(gpu.xya_GradLambda_wa(w), ora.xya_gradlambda_wa(w)),
+        "gradmu": relerr(gpu.xya_GradMu_wa(w), ora.xya_gradmu_wa(w)),
+        "gradlon": relerr(gpu.xya_GradLon_wa(w), ora.xya_gradlon_wa(w)),
+        "gradlat": relerr(gpu.xya_GradLat_wa(w), ora.xya_gradlat_wa(w)),
+        "divlambda": relerr(gpu.wa_DivLambda_xya(A), ora.wa_divlambda_xya(A)),
+        "divmu": relerr(gpu.wa_DivMu_xya(B), ora.wa_divmu_xya(B)),
+        "w_alpha": relerr(gpu.wa_AlphaOptr_xya(A, B), ora.wa_alphaoptr_xya(A, B)),
+        "xy_alpha": relerr(gpu.xya_AlphaOptr_wa(w, w2), ora.xya_alphaoptr_wa(w, w2)),
+        "lapla": relerr(gpu.w_Lapla_w(w), ora.wa_lapla_wa(w)),
+        "laplainv": relerr(gpu.w_LaplaInv_w(w), ora.wa_laplainv_wa(w)),
+    }
+    u, v = gpu.calc_VorDiv2UV(w / a, w2 / a)
+    uo, vo = ora.vordiv2uv(w / a, w2 / a)
+    res["U"], res["V"] = relerr(u, uo), relerr(v, vo)
+    vg, dg = gpu.calc_UVCosLat2VorDiv(A, B)
+    vr, dr = ora.uvcoslat2vordiv(A, B)
+    res["vor"], res["div"] = relerr(vg, vr), relerr(dg, dr)
+    bad = {k: v for k, v in res.items() if v > TOL}
+    assert not bad, bad
+
+
+def test_reductions_vs_oracle(plans):
+    gpu, ora = plans(128, 64, 42)
+    _, _, x = _inputs(128, 64, 42, 3)
+    # the means of random data cancel: measure the error against the data scale
+    scale = np.abs(x).mean()
+    assert np.abs(gpu.AvrLonLat_xy(x) - ora.avrlonlat(x)).max() / scale < 1e-14
+    assert np.abs(gpu.IntLonLat_xy(x) - ora.intlonlat(x)).max() / (4 * np.pi * scale) < 1e-14
+    assert np.abs(gpu.ya_AvrLon_xya(x) - ora.ya_avrlon(x)).max() / scale < 1e-14
+    assert np.abs(gpu.ya_IntLon_xya(x) - ora.ya_intlon(x)).max() / (2 * np.pi * scale) < 1e-14
+
+
+def test_grid_info_matches_oracle(plans):
+    gpu, ora = plans(256, 128, 85)
+    xl, yl, xw, yw = ora.grid_info()
+    assert np.abs(gpu.y_Lat - yl).max() < 1e-14
+    assert np.abs(gpu.y_Lat_Weight - yw).max() < 1e-15
+    assert np.abs(gpu.x_Lon - xl).max() == 0.0
+    assert abs(gpu.y_Lat_Weight.sum() - 2.0) < 1e-14
+    assert np.allclose(gpu.rn, ora.rn(), rtol=0, atol=0)
+
+
+def test_config_c0_full(plans):
+    """C0: T21, 20 levels x 3 fields: round trip plus gradient/divergence/vorticity."""
+    W = workloads()
+    c = W.CONFIGS["C0"]
+    I, J, N = W.GRIDS[c["grid"]]
+    nb = c["levels"] * c["fields"]
+    gpu, ora = plans(I, J, N, 6.371e6)
+    w = W.seeded_spectra(N, nb, c["power"])
+    g = gpu.xya_wa(w)
+    assert relerr(g, ora.xya_wa(w)) < TOL
+    assert relerr(gpu.wa_xya(g), w) < TOL
+    u, v = gpu.calc_VorDiv2UV(w / 6.371e6, w[::-1] / 6.371e6)
+    uo, vo = ora.vordiv2uv(w / 6.371e6, w[::-1] / 6.371e6)
+    assert relerr(u, uo) < TOL and relerr(v, vo) < TOL
+    cs = np.cos(gpu.y_Lat)[None, :, None]
+    vg, dg = gpu.calc_UVCosLat2VorDiv(u * cs, v * cs)
+    vr, dr = ora.uvcoslat2vordiv(u * cs, v * cs)
+    assert relerr(vg, vr) < TOL and relerr(dg, dr) < TOL
+
+
+def test_config_c1_tendency(plans):
+    """C1 pattern at T85 (HBEBaroc_HTRCRHS, HBEBaroc_hspm_vfvm_mod.f90:160-172): U,V from
+    vor/div, tracer gradients, grid products, analysed back by w_AlphaOptr_xy; 12 levels."""
+    W = workloads()
+    a = 6.371e6
+    I, J, N = W.GRIDS["T85"]
+    nb = 12
+    gpu, ora = plans(I, J, N, a)
+    vor = W.seeded_spectra(N, nb, 2.0, seed=1) / a
+    div = W.seeded_spectra(N, nb, 2.0, seed=2) / a
+    T = W.seeded_spectra(N, nb, 1.5, seed=3)
+    U, V = gpu.calc_VorDiv2UV(vor, div)
+    Uo, Vo = ora.vordiv2uv(vor, div)
+    Tg = gpu.xya_wa(T)
+    cs = np.cos(gpu.y_Lat)[None, :, None]
+    out = gpu.wa_AlphaOptr_xya(Tg * U * cs, Tg * V * cs)
+    ref = ora.wa_alphaoptr_xya(Tg * Uo * cs, Tg * Vo * cs)
+    assert relerr(U, Uo) < TOL and relerr(V, Vo) < TOL
+    assert relerr(out, ref) < TOL
+
+
+@pytest.mark.parametrize("grid", [(1024, 512, 341), (512, 256, 170)])
+def test_round_trip_property_large(grid, plans):
+    """Band-limited spectra survive synthesis + analysis (exact with J > N Gauss rows)."""
+    I, J, N = grid
+    gpu, _ = plans(I, J, N)
+    w = workloads().seeded_spectra(N, 8, 2.0)
+    assert relerr(gpu.wa_xya(gpu.xya_wa(w)), w) < TOL
+
+
+def test_device_pointer_path_matches_host(plans):
+    import torch
+    I, J, N = 256, 128, 85
+    gpu, _ = plans(I, J, N, 6.371e6)
+    w, w2, x = _inputs(I, J, N, 6)
+    wd = torch.from_numpy(w).cuda()
+    xd = torch.from_numpy(x).cuda()
+    assert np.array_equal(gpu.xya_wa(wd).cpu().numpy(), gpu.xya_wa(w))
+    assert np.array_equal(gpu.wa_xya(xd).cpu().numpy(), gpu.wa_xya(x))
+    u1, v1 = gpu.calc_VorDiv2UV(wd, torch.from_numpy(w2).cuda())
+    u2, v2 = gpu.calc_VorDiv2UV(w, w2)
+    assert np.array_equal(u1.cpu().numpy(), u2) and np.array_equal(v1.cpu().numpy(), v2)
+
+
+def test_single_level_and_odd_batches(plans):
+    gpu, ora = plans(128, 64, 42)
+    w, _, x = _inputs(128, 64, 42, 37)
+    assert relerr(gpu.xy_w(w[0])[None], ora.xya_wa(w[:1])) < TOL
+    assert relerr(gpu.wa_xya(x), ora.wa_xya(x)) < TOL  # 37 columns: ragged column tiles
+
+
+def test_diffusion_epilogue(plans):
+    import torch
+    W = workloads()
+    I, J, N = 256, 128, 85
+    gpu, ora = plans(I, J, N)
+    w = W.seeded_spectra(N, 4, 2.0)
+    coef = W.diffusion_coef(N, 8, 1e-3)
+    out = gpu.diffuse(w, coef, 1.0)
+    assert relerr(out, ora.diffuse(w, coef, 1.0)) < 1e-15
+    g = torch.from_numpy(gpu.xya_wa(w)).cuda().contiguous()
+    gpu.roundtrip_diffuse_(g, torch.from_numpy(coef).cuda(), 1.0)
+    ref = ora.xya_wa(ora.diffuse(ora.wa_xya(gpu.xya_wa(w)), coef, 1.0))
+    assert relerr(g.cpu().numpy(), ref) < TOL
+
+
+def test_error_paths(plans):
+    P = pkg()
+    gpu, _ = plans(64, 32, 21)
+    with pytest.raises(P.SpmlError):
+        gpu.xya_wa(np.zeros((2, 17)))
+    with pytest.raises(P.SpmlError):
+        gpu.set_precision(7)
+    g2 = P.SpmlUtil(64, 32, 1, 21, None, 1.0)
+    g2.final()
+    assert not g2.isInitialzed()
+    lib = P.load_library()
+    import ctypes
+    buf = (ctypes.c_double * 8)()
+    assert lib.sht_wa_xya(None, buf, 1, buf) == 3
