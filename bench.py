@@ -27,7 +27,6 @@ import importlib
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 
@@ -59,51 +58,69 @@ def _rel(a, b):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """Samples SM clock, max clock, power and clock-event reasons through NVML
+    every 100 ms in a background thread while the timed region runs."""
 
-    def __init__(self, gpu_id: str):
-        self.gpu_id = gpu_id
-        self.proc = None
-        self.path = os.path.join("/tmp", f"clocks_{os.getpid()}.csv")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+               ("hw_power_brake", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+
+    def __init__(self, props):
+        self.props = props
+        self.samples = []
+        self.reasons = set()
+        self.err = None
+        self._stop = None
+        self._thr = None
+
+    def _handle(self, nv):
+        p = self.props
+        bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        return nv.nvmlDeviceGetHandleByPciBusId(bus.encode())
 
     def start(self):
+        import threading
         try:
-            self.out = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", self.gpu_id, "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=self.out, stderr=subprocess.DEVNULL)
-        except Exception:
-            self.proc = None
+            import pynvml as nv
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        except Exception as ex:  # NVML missing: report it, do not guess
+            self.err = f"nvml unavailable: {ex}"
+            return
+        self._stop = threading.Event()
+
+        def run():
+            while not self._stop.is_set():
+                try:
+                    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                    pw = nv.nvmlDeviceGetPowerUsage(h) / 1000.0
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, pw))
+                    for name, const in self.REASONS:
+                        if r & getattr(nv, const, 0):
+                            self.reasons.add(name)
+                except Exception as ex:
+                    self.err = str(ex)
+                self._stop.wait(0.1)
+
+        self._thr = threading.Thread(target=run, daemon=True)
+        self._thr.start()
 
     def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        time.sleep(0.25)
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        self.out.close()
-        sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                smax.append(float(parts[1]))
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[4:8]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(smax) if smax else None,
-                "samples": len(sm), "reasons": sorted(reasons)}
+        if self._thr is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "samples": 0, "reasons": [self.err or "not sampled"]}
+        self._stop.set()
+        self._thr.join(timeout=2)
+        sm = [s for s, _ in self.samples]
+        pw = [p for _, p in self.samples]
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+               "samples": len(sm), "power_w_max": max(pw) if pw else None, "reasons": sorted(self.reasons)}
+        if self.err:
+            out["nvml_error"] = self.err
+        return out
 
 
 # ------------------------------------------------------------- reference
@@ -234,8 +251,7 @@ def main():
         barrier()
         torch.cuda.synchronize()
         n0 = P.launch_count()
-        clk = ClockSampler(str(torch.cuda.get_device_properties(dev).uuid)
-                           if hasattr(torch.cuda.get_device_properties(dev), "uuid") else str(local))
+        clk = ClockSampler(torch.cuda.get_device_properties(dev))
         clk.start()
         evs = []
         wall0 = time.perf_counter()
