@@ -59,7 +59,7 @@ def _rel(a, b):
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """Samples SM clock, max clock, power and clock-event reasons through NVML
-    every 100 ms in a background thread while the timed region runs."""
+    every 5 ms in a background thread while the timed region runs."""
 
     REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
@@ -104,7 +104,7 @@ class ClockSampler:
                             self.reasons.add(name)
                 except Exception as ex:
                     self.err = str(ex)
-                self._stop.wait(0.1)
+                self._stop.wait(0.005)
 
         self._thr = threading.Thread(target=run, daemon=True)
         self._thr.start()

@@ -1,0 +1,398 @@
+!> wa_module_b200 -- ISO_C_BINDING front end of libdogcm_sht.so for dogcm.
+!!
+!! It exports the SPMODEL wa_module names that SpmlUtil_mod re-exports
+!! (SpmlUtil_mod.f90:105-135), with the same dummy shapes, and routes every
+!! horizontal transform to the B200 library through the C-ABI of
+!! include/dogcm_sht.h.  It also exports fused forms of SpmlUtil_mod's
+!! composites (w_AlphaOptr_xy, calc_VorDiv2UV, ...) that take one library
+!! call instead of two to four SPMODEL calls.  Swap `use wa_module`
+!! (SpmlUtil_mod.f90:41-46) for `use wa_module_b200` to adopt it.
+!!
+!! Errors: every C entry point returns a status; a nonzero one is reported with
+!! MessageNotify('E', ...), which aborts, as the reference does on misuse.
+module wa_module_b200
+
+  use iso_c_binding
+  use dc_types, only: DP
+  use dc_message, only: MessageNotify
+
+  implicit none
+  private
+
+  public :: wa_Initial, wa_Finalize
+  public :: x_Lon, y_Lat, x_Lon_Weight, y_Lat_Weight, xy_Lon, xy_Lat
+  public :: rn, l_nm, nm_l
+  public :: w_xy, xy_w, wa_xya, xya_wa
+  public :: w_DivLambda_xy, w_DivMu_xy
+  public :: xy_GradLambda_w, xy_GradMu_w, xy_GradLon_w, xy_GradLat_w
+  public :: xya_GradLambda_wa, xya_GradMu_wa, xya_GradLon_wa, xya_GradLat_wa
+  public :: w_Lapla_w, w_LaplaInv_w
+  public :: AvrLonLat_xy, IntLonLat_xy, ya_AvrLon_xya, ya_IntLon_xya
+  public :: b200_wa_AlphaOptr_xya, b200_xya_AlphaOptr_wa
+  public :: b200_calc_UVCosLat2VorDiv, b200_calc_VorDiv2UV
+  public :: b200_wa_Diffuse
+
+  integer, parameter :: SHT_OK = 0
+  character(*), parameter :: module_name = 'wa_module_b200'
+
+  type(c_ptr), save :: plan = c_null_ptr
+  integer, save :: im = 0, jm = 0, nm = 0, lm = 0
+
+  real(DP), save, allocatable :: x_Lon(:), y_Lat(:), x_Lon_Weight(:), y_Lat_Weight(:)
+  real(DP), save, allocatable :: xy_Lon(:,:), xy_Lat(:,:)
+  real(DP), save, allocatable :: rn(:,:)
+
+  interface
+    integer(c_int) function sht_init(im, jm, km, nm, radius, plan) bind(C, name='sht_init')
+      import :: c_int, c_double, c_ptr
+      integer(c_int), value :: im, jm, km, nm
+      real(c_double), value :: radius
+      type(c_ptr), intent(out) :: plan
+    end function sht_init
+    integer(c_int) function sht_final(plan) bind(C, name='sht_final')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan
+    end function sht_final
+    integer(c_int) function sht_grid_info(plan, x_lon, y_lat, x_w, y_w) bind(C, name='sht_grid_info')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan
+      real(c_double), intent(out) :: x_lon(*), y_lat(*), x_w(*), y_w(*)
+    end function sht_grid_info
+    integer(c_int) function sht_rn(plan, rnv) bind(C, name='sht_rn')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan
+      real(c_double), intent(out) :: rnv(*)
+    end function sht_rn
+    function sht_last_error() bind(C, name='sht_last_error')
+      import :: c_ptr
+      type(c_ptr) :: sht_last_error
+    end function sht_last_error
+  end interface
+
+  ! One interface per entry point (each is a distinct C symbol).
+  interface
+    integer(c_int) function sht_wa_xya(plan, x, nb, w) bind(C, name='sht_wa_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_wa(plan, x, nb, w) bind(C, name='sht_xya_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_wa_divlambda_xya(plan, x, nb, w) bind(C, name='sht_wa_divlambda_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_wa_divmu_xya(plan, x, nb, w) bind(C, name='sht_wa_divmu_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_gradlambda_wa(plan, x, nb, w) bind(C, name='sht_xya_gradlambda_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_gradmu_wa(plan, x, nb, w) bind(C, name='sht_xya_gradmu_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_gradlon_wa(plan, x, nb, w) bind(C, name='sht_xya_gradlon_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_gradlat_wa(plan, x, nb, w) bind(C, name='sht_xya_gradlat_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_wa_lapla_wa(plan, x, nb, w) bind(C, name='sht_wa_lapla_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_wa_laplainv_wa(plan, x, nb, w) bind(C, name='sht_wa_laplainv_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_avrlonlat_xya(plan, x, nb, w) bind(C, name='sht_avrlonlat_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_intlonlat_xya(plan, x, nb, w) bind(C, name='sht_intlonlat_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_ya_avrlon_xya(plan, x, nb, w) bind(C, name='sht_ya_avrlon_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_ya_intlon_xya(plan, x, nb, w) bind(C, name='sht_ya_intlon_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_wa_alphaoptr_xya(plan, a, b, nb, w) bind(C, name='sht_wa_alphaoptr_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: a(*), b(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_alphaoptr_wa(plan, a, b, nb, x) bind(C, name='sht_xya_alphaoptr_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: a(*), b(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: x(*)
+    end function
+    integer(c_int) function sht_uvcoslat2vordiv(plan, u, v, nb, vor, div) bind(C, name='sht_uvcoslat2vordiv')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: u(*), v(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: vor(*), div(*)
+    end function
+    integer(c_int) function sht_vordiv2uv(plan, vor, div, nb, u, v) bind(C, name='sht_vordiv2uv')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: vor(*), div(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: u(*), v(*)
+    end function
+    integer(c_int) function sht_wa_diffuse(plan, w, nb, coef, dt, filt) bind(C, name='sht_wa_diffuse')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(inout) :: w(*)
+      integer(c_int), value :: nb; real(c_double), intent(in) :: coef(*)
+      real(c_double), value :: dt; real(c_double), intent(in) :: filt(*)
+    end function
+  end interface
+
+contains
+
+  subroutine check(status, where)
+    integer(c_int), intent(in) :: status
+    character(*), intent(in) :: where
+    character(kind=c_char), pointer :: msg(:)
+    character(len=256) :: text
+    integer :: k
+    if (status == SHT_OK) return
+    call c_f_pointer(sht_last_error(), msg, [256])
+    text = ''
+    do k = 1, 256
+       if (msg(k) == c_null_char) exit
+       text(k:k) = msg(k)
+    end do
+    call MessageNotify('E', module_name, trim(where)//': '//trim(text))
+  end subroutine check
+
+  !> wa_Initial(nm, im, jm, km[, np]) of SPMODEL (SpmlUtil_mod.f90:218-223); radius
+  !! is the planetary radius used by the fused composites (1 = unit sphere).
+  !! np (the SPMODEL OpenMP thread count) has no meaning on the GPU and is ignored.
+  subroutine wa_Initial(n_in, i_in, j_in, k_in, np, radius)
+    integer, intent(in) :: n_in, i_in, j_in, k_in
+    integer, intent(in), optional :: np
+    real(DP), intent(in), optional :: radius
+    real(DP) :: a
+    integer :: i, j
+    a = 1.0_DP
+    if (present(radius)) a = radius
+    nm = n_in; im = i_in; jm = j_in; lm = (nm + 1)**2
+    call check(sht_init(int(im, c_int), int(jm, c_int), int(k_in, c_int), int(nm, c_int), &
+         real(a, c_double), plan), 'wa_Initial')
+    allocate(x_Lon(0:im-1), y_Lat(jm), x_Lon_Weight(0:im-1), y_Lat_Weight(jm))
+    allocate(xy_Lon(0:im-1, jm), xy_Lat(0:im-1, jm), rn(lm, 2))
+    call check(sht_grid_info(plan, x_Lon, y_Lat, x_Lon_Weight, y_Lat_Weight), 'wa_Initial')
+    do j = 1, jm
+       do i = 0, im-1
+          xy_Lon(i, j) = x_Lon(i); xy_Lat(i, j) = y_Lat(j)
+       end do
+    end do
+    call check(sht_rn(plan, rn(:, 1)), 'wa_Initial')
+    rn(:, 2) = 0.0_DP  ! only rn(:,1), the Laplacian eigenvalue, is used by dogcm
+  end subroutine wa_Initial
+
+  subroutine wa_Finalize()
+    if (c_associated(plan)) call check(sht_final(plan), 'wa_Finalize')
+    plan = c_null_ptr
+    if (allocated(x_Lon)) deallocate(x_Lon, y_Lat, x_Lon_Weight, y_Lat_Weight, xy_Lon, xy_Lat, rn)
+  end subroutine wa_Finalize
+
+  integer function l_nm(n, m)
+    integer, intent(in) :: n, m
+    l_nm = n*(n + 1) + m + 1
+  end function l_nm
+
+  function nm_l(l)
+    integer, intent(in) :: l
+    integer :: nm_l(2), n
+    n = int(sqrt(real(l - 1, DP)))
+    do while ((n + 1)**2 <= l - 1); n = n + 1; end do
+    do while (n*n > l - 1); n = n - 1; end do
+    nm_l(1) = n; nm_l(2) = (l - 1) - n*(n + 1)
+  end function nm_l
+
+  function w_xy(xy)
+    real(DP), intent(in) :: xy(0:im-1, jm)
+    real(DP) :: w_xy(lm)
+    call check(sht_wa_xya(plan, xy, 1_c_int, w_xy), 'w_xy')
+  end function w_xy
+
+  function xy_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: xy_w(0:im-1, jm)
+    call check(sht_xya_wa(plan, w, 1_c_int, xy_w), 'xy_w')
+  end function xy_w
+
+  function wa_xya(xya)
+    real(DP), intent(in) :: xya(:,:,:)
+    real(DP) :: wa_xya(lm, size(xya, 3))
+    call check(sht_wa_xya(plan, xya, int(size(xya, 3), c_int), wa_xya), 'wa_xya')
+  end function wa_xya
+
+  function xya_wa(wa)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP) :: xya_wa(0:im-1, jm, size(wa, 2))
+    call check(sht_xya_wa(plan, wa, int(size(wa, 2), c_int), xya_wa), 'xya_wa')
+  end function xya_wa
+
+  function w_DivLambda_xy(xy)
+    real(DP), intent(in) :: xy(0:im-1, jm)
+    real(DP) :: w_DivLambda_xy(lm)
+    call check(sht_wa_divlambda_xya(plan, xy, 1_c_int, w_DivLambda_xy), 'w_DivLambda_xy')
+  end function w_DivLambda_xy
+
+  function w_DivMu_xy(xy)
+    real(DP), intent(in) :: xy(0:im-1, jm)
+    real(DP) :: w_DivMu_xy(lm)
+    call check(sht_wa_divmu_xya(plan, xy, 1_c_int, w_DivMu_xy), 'w_DivMu_xy')
+  end function w_DivMu_xy
+
+  function xy_GradLambda_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: xy_GradLambda_w(0:im-1, jm)
+    call check(sht_xya_gradlambda_wa(plan, w, 1_c_int, xy_GradLambda_w), 'xy_GradLambda_w')
+  end function xy_GradLambda_w
+
+  function xy_GradMu_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: xy_GradMu_w(0:im-1, jm)
+    call check(sht_xya_gradmu_wa(plan, w, 1_c_int, xy_GradMu_w), 'xy_GradMu_w')
+  end function xy_GradMu_w
+
+  function xy_GradLon_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: xy_GradLon_w(0:im-1, jm)
+    call check(sht_xya_gradlon_wa(plan, w, 1_c_int, xy_GradLon_w), 'xy_GradLon_w')
+  end function xy_GradLon_w
+
+  function xy_GradLat_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: xy_GradLat_w(0:im-1, jm)
+    call check(sht_xya_gradlat_wa(plan, w, 1_c_int, xy_GradLat_w), 'xy_GradLat_w')
+  end function xy_GradLat_w
+
+  function xya_GradLambda_wa(wa)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP) :: xya_GradLambda_wa(0:im-1, jm, size(wa, 2))
+    call check(sht_xya_gradlambda_wa(plan, wa, int(size(wa, 2), c_int), xya_GradLambda_wa), 'xya_GradLambda_wa')
+  end function xya_GradLambda_wa
+
+  function xya_GradMu_wa(wa)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP) :: xya_GradMu_wa(0:im-1, jm, size(wa, 2))
+    call check(sht_xya_gradmu_wa(plan, wa, int(size(wa, 2), c_int), xya_GradMu_wa), 'xya_GradMu_wa')
+  end function xya_GradMu_wa
+
+  function xya_GradLon_wa(wa)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP) :: xya_GradLon_wa(0:im-1, jm, size(wa, 2))
+    call check(sht_xya_gradlon_wa(plan, wa, int(size(wa, 2), c_int), xya_GradLon_wa), 'xya_GradLon_wa')
+  end function xya_GradLon_wa
+
+  function xya_GradLat_wa(wa)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP) :: xya_GradLat_wa(0:im-1, jm, size(wa, 2))
+    call check(sht_xya_gradlat_wa(plan, wa, int(size(wa, 2), c_int), xya_GradLat_wa), 'xya_GradLat_wa')
+  end function xya_GradLat_wa
+
+  function w_Lapla_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: w_Lapla_w(lm)
+    call check(sht_wa_lapla_wa(plan, w, 1_c_int, w_Lapla_w), 'w_Lapla_w')
+  end function w_Lapla_w
+
+  function w_LaplaInv_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: w_LaplaInv_w(lm)
+    call check(sht_wa_laplainv_wa(plan, w, 1_c_int, w_LaplaInv_w), 'w_LaplaInv_w')
+  end function w_LaplaInv_w
+
+  real(DP) function AvrLonLat_xy(xy)
+    real(DP), intent(in) :: xy(0:im-1, jm)
+    real(DP) :: r(1)
+    call check(sht_avrlonlat_xya(plan, xy, 1_c_int, r), 'AvrLonLat_xy')
+    AvrLonLat_xy = r(1)
+  end function AvrLonLat_xy
+
+  real(DP) function IntLonLat_xy(xy)
+    real(DP), intent(in) :: xy(0:im-1, jm)
+    real(DP) :: r(1)
+    call check(sht_intlonlat_xya(plan, xy, 1_c_int, r), 'IntLonLat_xy')
+    IntLonLat_xy = r(1)
+  end function IntLonLat_xy
+
+  function ya_AvrLon_xya(xya)
+    real(DP), intent(in) :: xya(:,:,:)
+    real(DP) :: ya_AvrLon_xya(jm, size(xya, 3))
+    call check(sht_ya_avrlon_xya(plan, xya, int(size(xya, 3), c_int), ya_AvrLon_xya), 'ya_AvrLon_xya')
+  end function ya_AvrLon_xya
+
+  function ya_IntLon_xya(xya)
+    real(DP), intent(in) :: xya(:,:,:)
+    real(DP) :: ya_IntLon_xya(jm, size(xya, 3))
+    call check(sht_ya_intlon_xya(plan, xya, int(size(xya, 3), c_int), ya_IntLon_xya), 'ya_IntLon_xya')
+  end function ya_IntLon_xya
+
+  ! ---- fused forms of SpmlUtil_mod's composites (one call for all levels)
+
+  !> wa_AlphaOptr_xya (SpmlUtil_mod.f90:453-473): (DivLambda(A) + DivMu(B)) / a
+  function b200_wa_AlphaOptr_xya(xya_A, xya_B)
+    real(DP), intent(in) :: xya_A(:,:,:), xya_B(:,:,:)
+    real(DP) :: b200_wa_AlphaOptr_xya(lm, size(xya_A, 3))
+    call check(sht_wa_alphaoptr_xya(plan, xya_A, xya_B, int(size(xya_A, 3), c_int), b200_wa_AlphaOptr_xya), &
+         'wa_AlphaOptr_xya')
+  end function b200_wa_AlphaOptr_xya
+
+  !> xya_AlphaOptr_wa (SpmlUtil_mod.f90:430-451): (GradLambda(A) + GradMu(B)) / (a cos^2 phi)
+  function b200_xya_AlphaOptr_wa(wa_A, wa_B)
+    real(DP), intent(in) :: wa_A(:,:), wa_B(:,:)
+    real(DP) :: b200_xya_AlphaOptr_wa(0:im-1, jm, size(wa_A, 2))
+    call check(sht_xya_alphaoptr_wa(plan, wa_A, wa_B, int(size(wa_A, 2), c_int), b200_xya_AlphaOptr_wa), &
+         'xya_AlphaOptr_wa')
+  end function b200_xya_AlphaOptr_wa
+
+  !> calc_UVCosLat2VorDiv_xya_wa (SpmlUtil_mod.f90:342-368)
+  subroutine b200_calc_UVCosLat2VorDiv(xya_UCosLat, xya_VCosLat, wa_Vor, wa_Div)
+    real(DP), intent(in) :: xya_UCosLat(:,:,:), xya_VCosLat(:,:,:)
+    real(DP), intent(out) :: wa_Vor(:,:), wa_Div(:,:)
+    call check(sht_uvcoslat2vordiv(plan, xya_UCosLat, xya_VCosLat, int(size(xya_UCosLat, 3), c_int), &
+         wa_Vor, wa_Div), 'calc_UVCosLat2VorDiv')
+  end subroutine b200_calc_UVCosLat2VorDiv
+
+  !> calc_VorDiv2UV_wa_xya (SpmlUtil_mod.f90:370-396)
+  subroutine b200_calc_VorDiv2UV(wa_Vor, wa_Div, xya_U, xya_V)
+    real(DP), intent(in) :: wa_Vor(:,:), wa_Div(:,:)
+    real(DP), intent(out) :: xya_U(:,:,:), xya_V(:,:,:)
+    call check(sht_vordiv2uv(plan, wa_Vor, wa_Div, int(size(wa_Vor, 2), c_int), xya_U, xya_V), 'calc_VorDiv2UV')
+  end subroutine b200_calc_VorDiv2UV
+
+  !> wa <- w_Filter * wa / (1 - dt c) (physics/DOGCM_Phys_hspm_vfvm_mod.f90:638-641, 741-742)
+  subroutine b200_wa_Diffuse(wa, coef, dt, w_Filter)
+    real(DP), intent(inout) :: wa(:,:)
+    real(DP), intent(in) :: coef(:), dt, w_Filter(:)
+    call check(sht_wa_diffuse(plan, wa, int(size(wa, 2), c_int), coef, real(dt, c_double), w_Filter), 'wa_Diffuse')
+  end subroutine b200_wa_Diffuse
+
+end module wa_module_b200
