@@ -210,6 +210,24 @@ SHT_API int sht_ya_intlon_xya_dev(sht_plan *plan, const double *xya, int nb, dou
 SHT_API int sht_roundtrip_diffuse_dev(sht_plan *plan, double *xya, int nb, const double *coef,
                               double dt, const double *filter);
 
+/* ------------------------------------------------- analysis without allocation */
+
+/* No counterpart in the reference: this entry point exists for callers that
+ * must not allocate device memory while they run.  Examples are a host whose
+ * GPU memory is owned by another pool allocator, a time loop that cannot
+ * absorb the device-wide synchronisation cudaMalloc/cudaFree may cause, or a
+ * policy of no allocation after start-up.  It computes the same result as
+ * sht_wa_xya_dev (w_xy / wa_xya on device arrays).  Its intermediate arrays
+ * live in one fixed device array of sht_noalloc_scratch_bytes() bytes
+ * (32 MiB), held by every GPU that loads the library until exit.  It calls no
+ * allocator.  A batch needing more scratch returns SHT_ERR_TOO_LARGE.  All
+ * calls share that array, so calls that overlap on the GPU race: order them
+ * on one stream.  The first call on each device looks up the array's address
+ * (cudaGetSymbolAddress), so make it before any stream capture.  The plan
+ * must already exist (sht_init allocates its tables). */
+SHT_API int sht_wa_xya_dev_noalloc(sht_plan *plan, const double *xya, int nb, double *wa);
+SHT_API unsigned long long sht_noalloc_scratch_bytes(void);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /* Device time in milliseconds of the kernels of the last *_dev call, summed
