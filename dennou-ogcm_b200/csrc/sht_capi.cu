@@ -301,7 +301,7 @@ void free_plan(sht_plan *p)
 {
   cudaFree(p->d_mu); cudaFree(p->d_wgt); cudaFree(p->d_rowscale); cudaFree(p->d_P);
   cudaFree(p->d_poff); cudaFree(p->d_rowoff); cudaFree(p->d_eps); cudaFree(p->d_tw);
-  cudaFree(p->d_twI); cudaFree(p->d_rn); cudaFree(p->d_spec_tiles);
+  cudaFree(p->d_twI); cudaFree(p->d_rn); cudaFree(p->d_spec_tiles); cudaFree(p->d_pairs);
   cudaFree(p->d_ws); cudaFree(p->d_io);
   free_split_tables(p);
   for (auto &ev : p->timing.ev)
@@ -460,6 +460,31 @@ int sht_get_precision(const sht_plan *p, int *mode)
   if (!mode) { set_error("NULL output"); return SHT_ERR_INVALID_ARG; }
   *mode = p->precision;
   return SHT_OK;
+}
+
+int sht_set_option(sht_plan *p, int option, int value)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  std::lock_guard<std::mutex> lk(p->mtx);
+  switch (option) {
+  case SHT_OPT_LEGENDRE_KERNEL:
+    if (value < 0 || value > 2) { set_error("legendre kernel option must be 0, 1 or 2"); return SHT_ERR_INVALID_ARG; }
+    p->leg_kernel = value;
+    return SHT_OK;
+  default: set_error("unknown option"); return SHT_ERR_INVALID_ARG;
+  }
+}
+
+int sht_get_option(const sht_plan *p, int option, int *value)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (!value) { set_error("NULL output"); return SHT_ERR_INVALID_ARG; }
+  switch (option) {
+  case SHT_OPT_LEGENDRE_KERNEL: *value = p->leg_kernel; return SHT_OK;
+  default: set_error("unknown option"); return SHT_ERR_INVALID_ARG;
+  }
 }
 
 int sht_set_stream(sht_plan *p, void *stream)

@@ -70,6 +70,7 @@ struct sht_plan_s {
   cudaStream_t stream = nullptr;      // stream used by all work of the plan
   cudaStream_t own_stream = nullptr;  // stream created by sht_init (destroyed by sht_final)
   int precision = SHT_PREC_FP64;
+  int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 chunked per-band, 2 paired persistent
 
   // device tables
   double *d_mu = nullptr, *d_wgt = nullptr, *d_rowscale = nullptr;
@@ -83,6 +84,9 @@ struct sht_plan_s {
   int2 *d_spec_tiles = nullptr;  // (n, m0) tiles of the spectral conversions
   int n_spec_tiles = 0;          // n = 0..N+1
   int n_pack_tiles = 0;          // n = 0..N (a prefix of the list)
+  int2 *d_pairs = nullptr;       // band pairs (m, N-m), (N/2, -1) for even N
+  int n_pairs = 0;
+  int num_sms = 0;
 
   // host copies
   std::vector<double> h_mu, h_wgt;
@@ -125,6 +129,11 @@ int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, in
 // --- Legendre contraction, FP64 (sht_legendre.cu)
 int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
+
+// --- persistent paired-band FP64 contraction (sht_legendre_v2.cu)
+bool leg_pair_supported(const sht_plan *p);
+int launch_leg_fwd_pair(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
+int launch_leg_inv_pair(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 
 // --- Legendre contraction, split precision on tcgen05 (sht_legendre_tc.cu)
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);

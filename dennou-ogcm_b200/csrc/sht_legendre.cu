@@ -330,6 +330,7 @@ int launch(K kern, dim3 grid, size_t smem, cudaStream_t s, const LegArgs &args, 
 int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
 {
   if (ncol <= 0) return SHT_OK;
+  if (p->leg_kernel != 1 && leg_pair_supported(p)) return launch_leg_fwd_pair(p, F, ncol, S, s);
   LegArgs a{};
   a.F = F; a.S = S; a.P = p->d_P; a.poff = p->d_poff; a.rowoff = p->d_rowoff;
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;
@@ -352,6 +353,7 @@ int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *
 int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s)
 {
   if (ncol <= 0) return SHT_OK;
+  if (p->leg_kernel != 1 && leg_pair_supported(p)) return launch_leg_inv_pair(p, S, ncol, F, s);
   LegArgs a{};
   a.Sc = S; a.Fo = F; a.P = p->d_P; a.poff = p->d_poff; a.rowoff = p->d_rowoff;
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;

@@ -1,0 +1,388 @@
+// sht_legendre_v2.cu -- persistent FP64 Legendre contraction with paired bands.
+//
+// The triangular band of order m has N+2-m degrees.  Pairing m with N-m makes
+// every pair hold N+4 degrees.  A work item is (pair, 16 complex field-level
+// columns), so all items cost the same.  Each thread block is resident and
+// takes a contiguous slice of the pair-major item list.  So it reloads the
+// pair's Legendre rows (P) at most a few times, and the blocks finish
+// together.  The next item's data panel is fetched with cp.async while the
+// current one is contracted on the FP64 tensor path (mma.sync.m8n8k4.f64).
+// Shared-memory row strides are chosen so that every 16-lane phase of a
+// fragment load touches 16 distinct double-word bank pairs:
+//   P rows (stride-2 rows of one parity):  PS = 2 (mod 8) doubles
+//   data rows (columns of one panel):      CS = 8 (mod 16) doubles
+//   coefficient rows (stride-2 rows):      AS = 2 (mod 8) doubles
+// Used when a pair's P rows and two data panels fit in shared memory (T85 and
+// smaller); larger grids use the chunked kernels of sht_legendre.cu.
+//
+// Analysis follows space_discretization.tex:197-200 and synthesis :212-216.
+// Symmetric and antisymmetric latitude halves use Pbar(-mu) = (-1)^{n-m} Pbar(mu).
+#include "sht_internal.h"
+
+namespace sht {
+
+namespace {
+
+constexpr int kW = 8;            // warps per block
+constexpr int kT = kW * 32;      // threads per block
+constexpr int kCT = 16;          // complex columns per item
+
+struct Geo {
+  int PS, CS, AS;      // strides (doubles)
+  int prow_cap;        // P rows reserved per pair (N+4 plus padding)
+  int arow_cap;        // coefficient rows reserved per m (rounded, zero tail)
+};
+
+__host__ __device__ inline int round_mod(int x, int r, int mod)
+{
+  while (x % mod != r) ++x;
+  return x;
+}
+
+__host__ __device__ inline Geo make_geo(int N, int J)
+{
+  Geo g;
+  const int JH = J / 2;
+  g.PS = round_mod(JH, 2, 8);
+  g.CS = round_mod(2 * J, 8, 16);
+  g.AS = round_mod(2 * kCT, 2, 8);
+  g.prow_cap = N + 4;
+  g.arow_cap = (N + 2 + 8 + 7) & ~7;  // rows of the larger band plus a zeroed tail (a k-step reads <= 5 past it)
+  return g;
+}
+
+struct V2Args {
+  const double2 *F;   // analysis input
+  double2 *S;         // analysis output
+  const double2 *Sc;  // synthesis input
+  double2 *Fo;        // synthesis output
+  const double *P;
+  const long long *poff;
+  const int *rowoff;
+  const int2 *pairs;  // (ma, mb), mb = -1 for a lone band
+  int ntiles, nitems, per_cta;
+  int N, J, JH, ncol;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void cp16(void *dst, const void *src, bool valid)
+{
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
+               "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+__device__ __forceinline__ void dmma(double (&d)[2], double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
+// Stage the Legendre rows of the pair: m_a rows at 0.., m_b rows right after.
+__device__ void load_pair_P(const V2Args &a, const Geo &g, double *Pbuf, int ma, int mb)
+{
+  const int Ra = a.N + 2 - ma, Rb = (mb >= 0) ? a.N + 2 - mb : 0;
+  const int cpr = a.JH / 2;  // 16-byte chunks per row
+  const int total = (Ra + Rb) * cpr;
+  const double *Pa = a.P + a.poff[ma];
+  const double *Pb = (mb >= 0) ? a.P + a.poff[mb] : Pa;
+  for (int q = threadIdx.x; q < total; q += kT) {
+    const int row = q / cpr, ch = q - row * cpr;
+    const double *src = (row < Ra) ? Pa + (long long)row * a.JH : Pb + (long long)(row - Ra) * a.JH;
+    cp16(Pbuf + row * g.PS + 2 * ch, src + 2 * ch, true);
+  }
+}
+
+// ------------------------------------------------------------------ analysis
+__device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
+{
+  const int nm = (mb >= 0) ? 2 : 1;
+  const int total = nm * kCT * a.J;
+  for (int q = threadIdx.x; q < total; q += kT) {
+    const int mi = q / (kCT * a.J), rem = q - mi * kCT * a.J;
+    const int b = rem / a.J, j = rem - b * a.J;
+    const int m = mi ? mb : ma;
+    const bool ok = col0 + b < a.ncol;
+    const double2 *src = ok ? a.F + ((long long)m * a.ncol + col0 + b) * a.J + j : a.F;
+    cp16(buf + (mi * kCT + b) * g.CS + 2 * j, src, ok);
+  }
+}
+
+// In place: row [j] of a column -> Gs at jh, Ga at JH + jh (jh = 0..JH-1)
+__device__ void combine_panels(const V2Args &a, const Geo &g, double *buf, int nm)
+{
+  const int JH = a.JH, half = JH / 2;
+  const int total = nm * kCT * half;
+  for (int q = threadIdx.x; q < total; q += kT) {
+    const int row = q / half, jh = q - row * half;
+    double2 *G = reinterpret_cast<double2 *>(buf + row * g.CS);
+    const int jq = JH - 1 - jh;
+    const double2 s0 = G[jh], s1 = G[jq];            // south rows JH-1-jq, JH-1-jh
+    const double2 n0 = G[JH + jh], n1 = G[JH + jq];  // north rows
+    G[jh] = make_double2(n0.x + s1.x, n0.y + s1.y);        // Gs(jh)  = G(JH+jh) + G(JH-1-jh)
+    G[jq] = make_double2(n1.x + s0.x, n1.y + s0.y);        // Gs(jq)
+    G[JH + jh] = make_double2(n0.x - s1.x, n0.y - s1.y);   // Ga(jh)
+    G[JH + jq] = make_double2(n1.x - s0.x, n1.y - s0.y);   // Ga(jq)
+  }
+}
+
+__global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
+{
+  extern __shared__ __align__(16) double sm[];
+  const Geo g = make_geo(a.N, a.J);
+  double *Pbuf = sm;
+  double *const G0 = sm + g.prow_cap * g.PS, *const G1 = G0 + 2 * kCT * g.CS;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int it0 = blockIdx.x * a.per_cta;
+  const int it1 = min(a.nitems, it0 + a.per_cta);
+  if (it0 >= it1) return;
+
+  {
+    const int2 pr = a.pairs[it0 / a.ntiles];
+    load_F_panels(a, g, G0, pr.x, pr.y, (it0 % a.ntiles) * kCT);
+    cp_commit();
+  }
+  int cur = -1;
+  for (int it = it0; it < it1; ++it) {
+    const int bsel = (it - it0) & 1;
+    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCT;
+    const int2 pr = a.pairs[pidx];
+    if (pidx != cur) {
+      load_pair_P(a, g, Pbuf, pr.x, pr.y);
+      cur = pidx;
+    }
+    cp_commit();
+    if (it + 1 < it1) {
+      const int2 pn = a.pairs[(it + 1) / a.ntiles];
+      load_F_panels(a, g, bsel ? G0 : G1, pn.x, pn.y, ((it + 1) % a.ntiles) * kCT);
+    }
+    cp_commit();
+    cp_wait1();
+    __syncthreads();
+    const int nm = (pr.y >= 0) ? 2 : 1;
+    double *const Gcur = bsel ? G1 : G0;
+    combine_panels(a, g, Gcur, nm);
+    __syncthreads();
+
+    // jobs: (band, parity, 16-row group)
+    const int Ra = a.N + 2 - pr.x, Rb = (pr.y >= 0) ? a.N + 2 - pr.y : 0;
+    const int gEa = ((Ra + 1) / 2 + 15) / 16, gOa = (Ra / 2 + 15) / 16;
+    const int gEb = ((Rb + 1) / 2 + 15) / 16, gOb = (Rb / 2 + 15) / 16;
+    const int njobs = gEa + gOa + gEb + gOb;
+    for (int job = warp; job < njobs; job += kW) {
+      int mi, par, gi;
+      if (job < gEa) { mi = 0; par = 0; gi = job; }
+      else if (job < gEa + gOa) { mi = 0; par = 1; gi = job - gEa; }
+      else if (job < gEa + gOa + gEb) { mi = 1; par = 0; gi = job - gEa - gOa; }
+      else { mi = 1; par = 1; gi = job - gEa - gOa - gEb; }
+      const int m = mi ? pr.y : pr.x, R = mi ? Rb : Ra;
+      const double *Pm = Pbuf + (mi ? Ra : 0) * g.PS;
+      const double *G = Gcur + mi * kCT * g.CS + (par ? 2 * a.JH : 0);
+      const int r0 = par + 2 * (16 * gi + (lane >> 2));
+      const int r1 = r0 + 16;
+      const double *pa0 = Pm + min(r0, R - 1) * g.PS + (lane & 3);
+      const double *pa1 = Pm + min(r1, R - 1) * g.PS + (lane & 3);
+      const double *gb = G + (lane >> 3) * g.CS + ((lane >> 2) & 1) + 2 * (lane & 3);
+      double acc[2][4][2];
+#pragma unroll
+      for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) acc[t][nt][0] = acc[t][nt][1] = 0.0;
+#pragma unroll 4
+      for (int kb = 0; kb < a.JH; kb += 4) {
+        const double a0 = pa0[kb], a1 = pa1[kb];
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const double b = gb[4 * nt * g.CS + 2 * kb];
+          dmma(acc[0][nt], a0, b);
+          dmma(acc[1][nt], a1, b);
+        }
+      }
+      const long long rowbase = a.rowoff[m];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        const int r = par + 2 * (16 * gi + 8 * t + (lane >> 2));
+        if (r >= R) continue;
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) {
+          const int c = col0 + 4 * nt + (lane & 3);
+          if (c < a.ncol) a.S[(rowbase + r) * a.ncol + c] = make_double2(acc[t][nt][0], acc[t][nt][1]);
+        }
+      }
+    }
+    __syncthreads();
+  }
+  cp_wait0();
+}
+
+// ----------------------------------------------------------------- synthesis
+__device__ void load_S_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
+{
+  const int nm = (mb >= 0) ? 2 : 1;
+  const int total = nm * g.arow_cap * kCT;
+  for (int q = threadIdx.x; q < total; q += kT) {
+    const int mi = q / (g.arow_cap * kCT), rem = q - mi * g.arow_cap * kCT;
+    const int r = rem / kCT, c = rem - r * kCT;
+    const int m = mi ? mb : ma;
+    const int R = a.N + 2 - m;
+    const bool ok = (r < R) && (col0 + c < a.ncol);
+    const double2 *src = ok ? a.Sc + ((long long)a.rowoff[m] + r) * a.ncol + col0 + c : a.Sc;
+    cp16(buf + (mi * g.arow_cap + r) * g.AS + 2 * c, src, ok);
+  }
+}
+
+__global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
+{
+  extern __shared__ __align__(16) double sm[];
+  const Geo g = make_geo(a.N, a.J);
+  double *Pbuf = sm;
+  const int abuf = 2 * g.arow_cap * g.AS;
+  double *const A0 = sm + g.prow_cap * g.PS, *const A1 = A0 + abuf;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int it0 = blockIdx.x * a.per_cta;
+  const int it1 = min(a.nitems, it0 + a.per_cta);
+  if (it0 >= it1) return;
+  // units: (latitude tile of 8, group of column tiles) over the 8 warps
+  const int ntj = a.JH / 8;               // 2, 4 or 8
+  const int ngrp = kW / ntj;              // 4, 2 or 1
+  const int nnt = 4 / ngrp;               // column tiles (of 8 reals) per unit
+  const int jt = warp % ntj, grp = warp / ntj;
+
+  {
+    const int2 pr = a.pairs[it0 / a.ntiles];
+    load_S_panels(a, g, A0, pr.x, pr.y, (it0 % a.ntiles) * kCT);
+    cp_commit();
+  }
+  int cur = -1;
+  for (int it = it0; it < it1; ++it) {
+    const int bsel = (it - it0) & 1;
+    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCT;
+    const int2 pr = a.pairs[pidx];
+    if (pidx != cur) {
+      load_pair_P(a, g, Pbuf, pr.x, pr.y);
+      cur = pidx;
+    }
+    cp_commit();
+    if (it + 1 < it1) {
+      const int2 pn = a.pairs[(it + 1) / a.ntiles];
+      load_S_panels(a, g, bsel ? A0 : A1, pn.x, pn.y, ((it + 1) % a.ntiles) * kCT);
+    }
+    cp_commit();
+    cp_wait1();
+    __syncthreads();
+
+    const int Ra = a.N + 2 - pr.x;
+    const int nm = (pr.y >= 0) ? 2 : 1;
+    for (int mi = 0; mi < nm; ++mi) {
+      const int m = mi ? pr.y : pr.x, R = a.N + 2 - m;
+      const double *Pm = Pbuf + (mi ? Ra : 0) * g.PS;
+      const double *A = (bsel ? A1 : A0) + mi * g.arow_cap * g.AS;
+      double acc[2][4][2];  // [parity][column tile][2]
+#pragma unroll
+      for (int p = 0; p < 2; ++p)
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) acc[p][nt][0] = acc[p][nt][1] = 0.0;
+      const int jcol = 8 * jt + (lane >> 2);
+#pragma unroll
+      for (int p = 0; p < 2; ++p) {
+        const int kp = (R - p + 1) / 2;  // rows of this parity
+        for (int t0 = 0; t0 < kp; t0 += 4) {
+          const int r = p + 2 * (t0 + (lane & 3));
+          const double av = Pm[min(r, R - 1) * g.PS + jcol];
+          const double *brow = A + r * g.AS + (lane >> 2);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < nnt) dmma(acc[p][q], av, brow[8 * (grp * nnt + q)]);
+        }
+      }
+      const int jh = 8 * jt + (lane >> 2);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        if (q >= nnt) continue;
+        const int c = col0 + 4 * (grp * nnt + q) + (lane & 3);
+        if (c >= a.ncol) continue;
+        double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * a.J;
+        const double er = acc[0][q][0], ei = acc[0][q][1], orr = acc[1][q][0], oi = acc[1][q][1];
+        Fc[a.JH + jh] = make_double2(er + orr, ei + oi);
+        Fc[a.JH - 1 - jh] = make_double2(er - orr, ei - oi);
+      }
+    }
+    __syncthreads();
+  }
+  cp_wait0();
+}
+
+size_t fwd_smem(int N, int J)
+{
+  const Geo g = make_geo(N, J);
+  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * 2 * kCT * (size_t)g.CS);
+}
+size_t inv_smem(int N, int J)
+{
+  const Geo g = make_geo(N, J);
+  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * 2 * (size_t)g.arow_cap * g.AS);
+}
+
+int get_pairs(const sht_plan *p, const int2 **out, int *n)
+{
+  // The pair list is a pure function of N; it is kept per plan in d_pairs.
+  *out = p->d_pairs;
+  *n = p->n_pairs;
+  return (p->d_pairs && p->n_pairs > 0) ? SHT_OK : SHT_ERR_NOT_INITIALIZED;
+}
+
+int launch_pair(const sht_plan *p, bool inverse, const double2 *in, int ncol, double2 *out, cudaStream_t s)
+{
+  V2Args a{};
+  if (inverse) { a.Sc = in; a.Fo = out; } else { a.F = in; a.S = out; }
+  a.P = p->d_P; a.poff = p->d_poff; a.rowoff = p->d_rowoff;
+  a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;
+  int npairs = 0;
+  int rc = get_pairs(p, &a.pairs, &npairs);
+  if (rc) { set_error("legendre: pair table missing"); return rc; }
+  a.ntiles = (ncol + kCT - 1) / kCT;
+  a.nitems = npairs * a.ntiles;
+  const size_t smem = inverse ? inv_smem(p->N, p->J) : fwd_smem(p->N, p->J);
+  auto kern = inverse ? k_leg_inv_pair : k_leg_fwd_pair;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return cuda_fail(e, "legendre pair smem attribute");
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, smem);
+  if (e != cudaSuccess || per_sm < 1) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidConfiguration : e, "legendre pair occupancy");
+  const int slots = p->num_sms * per_sm;
+  a.per_cta = (a.nitems + slots - 1) / slots;
+  const int grid = (a.nitems + a.per_cta - 1) / a.per_cta;
+  kern<<<grid, kT, smem, s>>>(a);
+  count_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_leg_inv_pair" : "k_leg_fwd_pair");
+}
+
+}  // namespace
+
+bool leg_pair_supported(const sht_plan *p)
+{
+  if (p->J % 16 != 0 || (p->JH != 16 && p->JH != 32 && p->JH != 64)) return false;
+  const size_t lim = 227 * 1024;
+  return fwd_smem(p->N, p->J) <= lim && inv_smem(p->N, p->J) <= lim;
+}
+
+int launch_leg_fwd_pair(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
+{
+  if (ncol <= 0) return SHT_OK;
+  return launch_pair(p, false, F, ncol, S, s);
+}
+
+int launch_leg_inv_pair(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s)
+{
+  if (ncol <= 0) return SHT_OK;
+  return launch_pair(p, true, S, ncol, F, s);
+}
+
+}  // namespace sht

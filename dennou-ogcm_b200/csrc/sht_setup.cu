@@ -191,6 +191,16 @@ int build_tables(sht_plan *p)
     for (int m0 = 0; m0 <= mmax; m0 += 32) tiles.push_back(make_int2(n, m0));
   }
   p->n_spec_tiles = (int)tiles.size();
+  // --- band pairs (m, N-m) with N+4 degrees each, plus the middle band of even N
+  std::vector<int2> pairs;
+  for (int m = 0; m < N - m; ++m) pairs.push_back(make_int2(m, N - m));
+  if (N % 2 == 0) pairs.push_back(make_int2(N / 2, -1));
+  p->n_pairs = (int)pairs.size();
+  if ((rc = dalloc(&p->d_pairs, pairs.size()))) return rc;
+  if ((e = cudaMemcpyAsync(p->d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, p->stream)) != cudaSuccess)
+    return cuda_fail(e, "pair table upload");
+  if ((e = cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, p->device)) != cudaSuccess)
+    return cuda_fail(e, "SM count");
   if ((rc = dalloc(&p->d_spec_tiles, tiles.size()))) return rc;
   if ((e = cudaMemcpyAsync(p->d_spec_tiles, tiles.data(), sizeof(int2) * tiles.size(), cudaMemcpyHostToDevice, p->stream)) != cudaSuccess)
     return cuda_fail(e, "spectral tiles upload");

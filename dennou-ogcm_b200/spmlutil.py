@@ -29,6 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libdogcm_sht.so")
 SHT_OK = 0
 SHT_PREC_FP64 = 0
 SHT_PREC_SPLIT = 1
+SHT_OPT_LEGENDRE_KERNEL = 1
 
 _D = ctypes.POINTER(ctypes.c_double)
 _VP = ctypes.c_void_p
@@ -75,6 +76,8 @@ def load_library(path: str | None = None):
     lib.sht_set_precision.argtypes = [_VP, ctypes.c_int]
     lib.sht_get_precision.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
     lib.sht_set_stream.argtypes = [_VP, _VP]
+    lib.sht_set_option.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
+    lib.sht_get_option.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.sht_synchronize.argtypes = [_VP]
     lib.sht_set_timing.argtypes = [_VP, ctypes.c_int]
     lib.sht_last_timing.argtypes = [_VP] + [ctypes.POINTER(ctypes.c_float)] * 3
@@ -183,6 +186,14 @@ class SpmlUtil:
         m = ctypes.c_int()
         _check(load_library().sht_get_precision(self._h, ctypes.byref(m)), "get_precision")
         return m.value
+
+    def set_option(self, option: int, value: int):
+        _check(load_library().sht_set_option(self._h, int(option), int(value)), "set_option")
+
+    def get_option(self, option: int) -> int:
+        v = ctypes.c_int()
+        _check(load_library().sht_get_option(self._h, int(option), ctypes.byref(v)), "get_option")
+        return v.value
 
     def set_timing(self, on: bool):
         _check(load_library().sht_set_timing(self._h, int(bool(on))), "set_timing")

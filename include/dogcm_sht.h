@@ -105,6 +105,14 @@ SHT_API int sht_rn(const sht_plan *plan, double *rn);
 SHT_API int sht_set_precision(sht_plan *plan, int mode);
 SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
 
+/* Kernel choices (used by the autotuner and the tests; the defaults are
+ * picked per grid).  SHT_OPT_LEGENDRE_KERNEL: 0 automatic, 1 per-band chunked
+ * kernel (any grid), 2 persistent paired-band kernel (T85 and smaller; falls
+ * back to 1 where it does not fit). */
+#define SHT_OPT_LEGENDRE_KERNEL 1
+SHT_API int sht_set_option(sht_plan *plan, int option, int value);
+SHT_API int sht_get_option(const sht_plan *plan, int option, int *value);
+
 /* Stream for the *_dev calls (a cudaStream_t passed as void*; NULL = legacy
  * default stream), and a wait for all work on it. */
 SHT_API int sht_set_stream(sht_plan *plan, void *stream);
