@@ -293,6 +293,7 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
   if (sh.nout == 2 && (e = cudaMemcpyAsync(o1, do1, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_fail(e, "D2H");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
+  if (p->precision == SHT_PREC_SPLIT && (rc = split_error_status(p))) return rc;
   finish_timing(p, !sh.out_grid);
   return SHT_OK;
 }
@@ -502,7 +503,8 @@ int sht_synchronize(sht_plan *p)
   if (rc) return rc;
   DeviceGuard g(p->device);
   cudaError_t e = cudaStreamSynchronize(p->stream);
-  return e == cudaSuccess ? SHT_OK : cuda_fail(e, "synchronize");
+  if (e != cudaSuccess) return cuda_fail(e, "synchronize");
+  return split_error_status(p);
 }
 
 int sht_set_timing(sht_plan *p, int on)

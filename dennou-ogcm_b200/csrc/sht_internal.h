@@ -139,6 +139,8 @@ int launch_leg_inv_pair(const sht_plan *p, const double2 *S, int ncol, double2 *
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_split(sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 void free_split_tables(sht_plan *p);
+bool split_supported(const sht_plan *p);
+int split_error_status(sht_plan *p);  // reads and clears the device error word (synchronous)
 
 // --- spectral-side kernels (sht_spectral.cu)
 // internal S (ncolS columns; set A at col 0, set B at col nb) -> SPML wa outputs

@@ -1,0 +1,100 @@
+"""Split-precision Legendre contraction (BF16 digit products on tcgen05, FP64
+recombination) through the C-ABI, against the CPU oracle and the FP64 path.
+
+Tolerance: 1e-11 per-field normwise relative error, the same bar as the plain
+FP64 path (the error-free splitting keeps about 46 bits per operand).
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import pkg, relerr, workloads
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+GRIDS = [(64, 32, 21), (128, 64, 42), (256, 128, 85)]
+
+
+@pytest.fixture(scope="module")
+def plan_cache():
+    cache = {}
+
+    def get(I, J, N, a=1.0):
+        key = (I, J, N, a)
+        if key not in cache:
+            cache[key] = (pkg().SpmlUtil(I, J, 1, N, None, a), O.OraclePlan(I, J, N, a))
+        return cache[key]
+
+    yield get
+    for g, _ in cache.values():
+        g.final()
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_split_round_trip_vs_oracle(grid, plan_cache):
+    P, W = pkg(), workloads()
+    I, J, N = grid
+    gpu, ora = plan_cache(I, J, N)
+    rng = np.random.default_rng(5)
+    w = W.seeded_spectra(N, 70, 2.0, rng=rng)      # 70 columns: a ragged 64-column tile
+    x = rng.standard_normal((70, J, I))
+    gpu.set_precision(P.SHT_PREC_SPLIT)
+    try:
+        g_split = gpu.xya_wa(w)
+        w_split = gpu.wa_xya(x)
+        gpu.synchronize()  # also reads the device error word of the bounded waits
+    finally:
+        gpu.set_precision(P.SHT_PREC_FP64)
+    assert relerr(g_split, ora.xya_wa(w)) < TOL
+    assert relerr(w_split, ora.wa_xya(x)) < TOL
+    assert relerr(g_split, gpu.xya_wa(w)) < TOL
+
+
+@pytest.mark.parametrize("grid", GRIDS)
+def test_split_derivatives_vs_oracle(grid, plan_cache):
+    P, W = pkg(), workloads()
+    I, J, N = grid
+    a = 6.371e6
+    gpu, ora = plan_cache(I, J, N, a)
+    w = W.seeded_spectra(N, 9, 2.0, seed=3) / a
+    w2 = W.seeded_spectra(N, 9, 2.0, seed=4) / a
+    gpu.set_precision(P.SHT_PREC_SPLIT)
+    try:
+        u, v = gpu.calc_VorDiv2UV(w, w2)
+        cs = np.cos(gpu.y_Lat)[None, :, None]
+        vo, di = gpu.calc_UVCosLat2VorDiv(u * cs, v * cs)
+        gpu.synchronize()
+    finally:
+        gpu.set_precision(P.SHT_PREC_FP64)
+    uo, vvo = ora.vordiv2uv(w, w2)
+    vr, dr = ora.uvcoslat2vordiv(u * cs, v * cs)
+    assert relerr(u, uo) < TOL and relerr(v, vvo) < TOL
+    assert relerr(vo, vr) < TOL and relerr(di, dr) < TOL
+
+
+def test_split_t85_full_batch_round_trip(plan_cache):
+    """The benchmark batch (480 field-levels at T85) survives a split round trip."""
+    P, W = pkg(), workloads()
+    I, J, N = W.GRIDS["T85"]
+    gpu, _ = plan_cache(I, J, N)
+    w = W.seeded_spectra(N, 480, 2.0)
+    gpu.set_precision(P.SHT_PREC_SPLIT)
+    try:
+        out = gpu.wa_xya(gpu.xya_wa(w))
+        gpu.synchronize()
+    finally:
+        gpu.set_precision(P.SHT_PREC_FP64)
+    assert relerr(out, w) < TOL
+
+
+def test_split_rejects_grids_it_does_not_cover(plan_cache):
+    P = pkg()
+    gpu, _ = plan_cache(512, 256, 170)
+    gpu.set_precision(P.SHT_PREC_SPLIT)
+    try:
+        with pytest.raises(P.SpmlError) as ei:
+            gpu.xya_wa(np.zeros((1, gpu.lm)))
+        assert ei.value.status == 2
+    finally:
+        gpu.set_precision(P.SHT_PREC_FP64)
