@@ -15,15 +15,23 @@
 // residual is below 2^-56 of its row or column maximum), and the dropped
 // products are below 2^-62.
 //
-// Layout of one CTA (128 threads, one per real data column):
-//   M = 128 data columns (64 complex field-levels), N = rows of one parity
-//   (analysis) or Gauss rows (synthesis), K = 64 per chunk.  A (data digits)
-//   and B (table digits) are K-major, in the interleaved canonical layout
-//   (8-row x 16-byte core matrices, LBO = 128 B along K, SBO = 1024 B across
-//   row groups).  D is FP32 in TMEM, lane = data column.  One thread issues
-//   the MMAs and commits them to an mbarrier.  Waits are bounded: a timeout
-//   sets the plan's device error word and the kernel unwinds (frees TMEM).
-//
+// Kernel organisation (one resident CTA of 256 threads per SM):
+//   * Work item = (band pair (m, N-m), 64 complex field-level columns).  The
+//     pair keeps every item about the same cost.  An item has up to four
+//     sub-items (m, parity) and each sub-item has K chunks of 32.
+//   * The data digits of chunk u+1 (and its table digits) are written into
+//     the other of two shared-memory stages while the tensor core runs the
+//     asynchronous MMAs of chunk u, issued by one thread.
+//   * When a sub-item's last chunk completes, all threads read its seven
+//     TMEM levels, 16 columns at a time (the two warp halves take alternate
+//     groups), and recombine them in FP64.
+//   * M = 128 data columns (re/im of 64 field-levels; TMEM lane = column).
+//     N = degrees of one parity (analysis) or Gauss rows (synthesis).
+//     A and B are K-major in the interleaved canonical layout (8-row x
+//     16-byte core matrices, LBO = 128 B along K, SBO = 512 B across row
+//     groups).
+//   * Every wait is bounded in time.  A timeout sets the plan's device error
+//     word, and the kernel unwinds and frees its TMEM.
 // The table digits are built once per plan on the device (k_slice_table_*).
 // Follows space_discretization.tex:197-200 (analysis) and :212-216 (synthesis).
 #include "sht_internal.h"
@@ -36,19 +44,20 @@ namespace sht {
 
 namespace {
 
-constexpr int kS = 7;             // digits per operand
-constexpr int kKC = 64;           // K per chunk (4 MMA K-steps of 16)
-constexpr int kM = 128;           // data columns per CTA (64 complex)
-constexpr int kTileBytesPerRow = kKC * 2;  // 128 B per row of one digit tile
+constexpr int kS = 7;                      // digits per operand
+constexpr int kKC = 32;                    // K per chunk (2 MMA K-steps of 16)
+constexpr int kM = 128;                    // data columns per CTA (64 complex)
+constexpr int kRowB = kKC * 2;             // 64 bytes per row of one digit tile
+constexpr int kThreads = 256;
 constexpr uint64_t kWaitLimit = 2000000000ull;  // 2 s per bounded wait
 
-// byte offset of element (row, k) inside a canonical K-major tile of 64 k
+// byte offset of element (row, k) inside a canonical K-major tile of 32 k
 __host__ __device__ inline uint32_t canon(int row, int k)
 {
-  return (uint32_t)((row >> 3) * 1024 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
+  return (uint32_t)((row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-__device__ __forceinline__ void digits6(double x, float (&d)[kS])
+__device__ __forceinline__ void digits(double x, float (&d)[kS])
 {
   // x in (-1, 1): balanced digits, d0 in [-128,128], |r| <= 1/2 after each step,
   // so |x - sum_s d_s 2^{-7-8s}| <= 2^{-7-8 kS}
@@ -61,22 +70,24 @@ __device__ __forceinline__ void digits6(double x, float (&d)[kS])
   }
 }
 
-struct SplitTables {
-  // analysis operand B: per (m, p): rows = degrees of parity p, K = latitudes
-  __nv_bfloat16 *fwd = nullptr;
-  long long *fwd_off = nullptr;  // element offset per (m,p)
-  int *fwd_exp = nullptr;        // exponent per row
-  int *fwd_eoff = nullptr;       // row offset per (m,p) into fwd_exp
-  int *fwd_npad = nullptr;       // padded rows per (m,p)
-  // synthesis operand B: per (m, p): rows = latitudes, K = degrees of parity p
-  __nv_bfloat16 *inv = nullptr;
-  long long *inv_off = nullptr;
-  int *inv_exp = nullptr;        // exponent per latitude, per (m,p): [m*2+p][JH]
-  int *inv_kch = nullptr;        // K chunks per (m,p)
-  int npad_max = 0;
-  int *d_err = nullptr;          // device error word
-  int fwd_kch = 0;               // K chunks of the analysis (latitudes)
-};
+// The same digits as BF16 bit patterns without conversion instructions:
+// adding 1.5*2^52 rounds |v| < 2^51 to the nearest integer, which lands in the
+// low word; an integer d with |d| <= 128 becomes an exact FP32 value through
+// 1.5*2^23 + d, whose top 16 bits are its BF16 encoding.
+__device__ __forceinline__ void digits_bf16(double x, unsigned short (&h)[kS])
+{
+  const double M52 = 6755399441055744.0;  // 1.5 * 2^52
+  double v = x * 128.0;
+#pragma unroll
+  for (int s = 0; s < kS; ++s) {
+    const double t = v + M52;
+    const int di = __double2loint(t);
+    const double q = t - M52;
+    v = (v - q) * 256.0;
+    const float f = __int_as_float(0x4B400000 + di) - 12582912.0f;
+    h[s] = (unsigned short)(__float_as_uint(f) >> 16);
+  }
+}
 
 __host__ __device__ inline int rows_of_parity(int N, int m, int p)
 {
@@ -85,37 +96,52 @@ __host__ __device__ inline int rows_of_parity(int N, int m, int p)
 }
 __host__ __device__ inline int round_up(int x, int r) { return (x + r - 1) / r * r; }
 
+struct SplitTables {
+  // analysis operand B per (m, p): rows = degrees of parity p, K = latitudes
+  __nv_bfloat16 *fwd = nullptr;
+  long long *fwd_off = nullptr;  // element offset per (m,p)
+  int *fwd_exp = nullptr;        // exponent per row
+  int *fwd_eoff = nullptr;       // row offset per (m,p) into fwd_exp
+  int fwd_npad_max = 0;
+  // synthesis operand B per (m, p): rows = latitudes, K = degrees of parity p
+  __nv_bfloat16 *inv = nullptr;
+  long long *inv_off = nullptr;
+  int *inv_exp = nullptr;        // exponent per latitude: [m*2+p][JH]
+  int inv_npad = 0;
+  int *d_err = nullptr;          // device error word
+};
+
 // one thread per (m, p, row i): digits of Pbar_{m+p+2i}^m over the latitudes
 __global__ void k_slice_table_fwd(int N, int JH, const double *__restrict__ P, const long long *__restrict__ poff,
                                   __nv_bfloat16 *tab, const long long *__restrict__ off, int *exps,
-                                  const int *__restrict__ eoff, const int *__restrict__ npad, int kch)
+                                  const int *__restrict__ eoff)
 {
   const int mp = blockIdx.y, m = mp >> 1, p = mp & 1;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (m > N || i >= rows_of_parity(N, m, p)) return;
+  const int Rp = rows_of_parity(N, m, p);
+  if (m > N || i >= Rp) return;
+  const int np = round_up(Rp, 16);
   const double *row = P + poff[m] + (long long)(p + 2 * i) * JH;
   double mx = 0.0;
   for (int k = 0; k < JH; ++k) mx = fmax(mx, fabs(row[k]));
   int e = 0;
   frexp(mx, &e);
   exps[eoff[mp] + i] = e;
-  const int np = npad[mp];
   for (int k = 0; k < JH; ++k) {
     float d[kS];
-    digits6(ldexp(row[k], -e), d);
-    const int kc = k / kKC, kk = k % kKC;
+    digits(ldexp(row[k], -e), d);
+    const int h = k / kKC, kk = k % kKC;
 #pragma unroll
     for (int s = 0; s < kS; ++s) {
-      char *tile = reinterpret_cast<char *>(tab + off[mp]) + ((size_t)(kc * kS + s) * np) * kTileBytesPerRow;
+      char *tile = reinterpret_cast<char *>(tab + off[mp]) + ((size_t)(h * kS + s) * np) * kRowB;
       *reinterpret_cast<__nv_bfloat16 *>(tile + canon(i, kk)) = __float2bfloat16_rn(d[s]);
     }
   }
-  (void)kch;
 }
 
 // one thread per (m, p, latitude jh): digits of Pbar_{m+p+2i}^m over the degrees i
 __global__ void k_slice_table_inv(int N, int JH, const double *__restrict__ P, const long long *__restrict__ poff,
-                                  __nv_bfloat16 *tab, const long long *__restrict__ off, int *exps, int npad_rows)
+                                  __nv_bfloat16 *tab, const long long *__restrict__ off, int *exps, int np)
 {
   const int mp = blockIdx.y, m = mp >> 1, p = mp & 1;
   const int jh = blockIdx.x * blockDim.x + threadIdx.x;
@@ -129,11 +155,11 @@ __global__ void k_slice_table_inv(int N, int JH, const double *__restrict__ P, c
   exps[mp * JH + jh] = e;
   for (int i = 0; i < Rp; ++i) {
     float d[kS];
-    digits6(ldexp(base[(long long)(p + 2 * i) * JH], -e), d);
-    const int kc = i / kKC, kk = i % kKC;
+    digits(ldexp(base[(long long)(p + 2 * i) * JH], -e), d);
+    const int h = i / kKC, kk = i % kKC;
 #pragma unroll
     for (int s = 0; s < kS; ++s) {
-      char *tile = reinterpret_cast<char *>(tab + off[mp]) + ((size_t)(kc * kS + s) * npad_rows) * kTileBytesPerRow;
+      char *tile = reinterpret_cast<char *>(tab + off[mp]) + ((size_t)(h * kS + s) * np) * kRowB;
       *reinterpret_cast<__nv_bfloat16 *>(tile + canon(jh, kk)) = __float2bfloat16_rn(d[s]);
     }
   }
@@ -145,22 +171,70 @@ struct TcArgs {
   const double2 *Sc;  // synthesis input
   double2 *Fo;        // synthesis output
   const int *rowoff;
+  const int2 *pairs;
   const __nv_bfloat16 *tab;
   const long long *toff;
   const int *texp;
   const int *teoff;   // analysis: row-exponent offsets
-  const int *tnpad;   // analysis: padded rows
-  int N, J, JH, ncol, fwd_kch;
+  int N, J, JH, ncol;
+  int ntiles, nitems, per_cta;
+  int npad_max;       // TMEM columns per level
   int *err;
 };
 
-// Issue the 21 digit-pair MMAs of one K chunk into D_L = tbase + L*ncols_per_level.
-__device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_t a_base, uint32_t b_base,
-                                            int npad, bool first_chunk)
+// Sub-item bookkeeping shared by both directions.
+struct Sub {
+  int m, p, Rp, npad, nch, slot;
+};
+
+template <bool INV>
+__device__ __forceinline__ Sub make_sub(const TcArgs &a, int m, int p, int q)
+{
+  Sub s;
+  s.m = m;
+  s.p = p;
+  s.Rp = rows_of_parity(a.N, m, p);
+  s.npad = INV ? a.npad_max : round_up(s.Rp, 16);
+  s.nch = INV ? (s.Rp + kKC - 1) / kKC : (a.JH + kKC - 1) / kKC;
+  s.slot = q & 3;
+  return s;
+}
+
+// Unit iterator: (item, sub-item, chunk) in order, uniform across the CTA.
+struct Cursor {
+  int it, sub, h, q;  // item, sub-item index within the item, chunk, running sub-item count
+};
+
+template <bool INV>
+__device__ __forceinline__ void cursor_sub(const TcArgs &a, const Cursor &c, Sub &out)
+{
+  const int2 pr = a.pairs[c.it / a.ntiles];
+  const int m = (c.sub < 2) ? pr.x : pr.y;
+  out = make_sub<INV>(a, m, c.sub & 1, c.q);
+}
+
+template <bool INV>
+__device__ __forceinline__ void cursor_next(const TcArgs &a, Cursor &c)
+{
+  Sub s;
+  cursor_sub<INV>(a, c, s);
+  if (++c.h < s.nch) return;
+  c.h = 0;
+  ++c.q;
+  const int2 pr = a.pairs[c.it / a.ntiles];
+  const int nsub = (pr.y >= 0) ? 4 : 2;
+  if (++c.sub < nsub) return;
+  c.sub = 0;
+  ++c.it;
+}
+
+// Issue the 28 digit-pair MMAs of one K chunk into D_L = tbase + L*dstride.
+__device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_t a_base, uint32_t b_base, int npad,
+                                            bool first_chunk)
 {
   const uint32_t idesc = tc::idesc_bf16_f32(kM, npad);
-  const uint32_t a_tile = kM * kTileBytesPerRow;   // bytes per digit tile of A
-  const uint32_t b_tile = npad * kTileBytesPerRow; // bytes per digit tile of B
+  const uint32_t a_tile = kM * kRowB;    // bytes per digit tile of A
+  const uint32_t b_tile = npad * kRowB;  // bytes per digit tile of B
 #pragma unroll
   for (int L = 0; L < kS; ++L) {
 #pragma unroll
@@ -168,8 +242,8 @@ __device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_
       const int t = L - s;
 #pragma unroll
       for (int ks = 0; ks < kKC / 16; ++ks) {
-        const uint64_t ad = tc::smem_desc(a_base + s * a_tile + ks * 256, 128, 1024);
-        const uint64_t bd = tc::smem_desc(b_base + t * b_tile + ks * 256, 128, 1024);
+        const uint64_t ad = tc::smem_desc(a_base + s * a_tile + ks * 256, 128, 512);
+        const uint64_t bd = tc::smem_desc(b_base + t * b_tile + ks * 256, 128, 512);
         const uint32_t acc = (first_chunk && s == 0 && ks == 0) ? 0u : 1u;
         tc::mma_bf16(tbase + (uint32_t)(L * dstride), ad, bd, idesc, acc);
       }
@@ -177,257 +251,291 @@ __device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_
   }
 }
 
-// ------------------------------------------------------------------ analysis
-template <int NPAD>
-__global__ void __launch_bounds__(128, 1) k_leg_fwd_split(TcArgs a)
+struct Smem {
+  unsigned char *A[2];
+  unsigned char *B[2];
+  int *exps;      // [4 slots][128 columns]
+  double *part;   // [2][2][128] partial maxima
+};
+
+// Column exponents of the sub-items that start at this chunk.
+template <bool INV>
+__device__ void column_exponents(const TcArgs &a, const Sub &s, int col0, const Smem &sm)
 {
-  extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ uint64_t mbar;
-  __shared__ uint32_t tslot;
-  unsigned char *Asm = smem;                              // kS x 128 x 64 bf16 = 96 KB
-  unsigned char *Bsm = smem + kS * kM * kTileBytesPerRow; // kS x NPAD x 64 bf16
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const int m = blockIdx.y, col0 = blockIdx.x * (kM / 2);
-  const int b = col0 + (tid >> 1), part = tid & 1;
+  const int tid = threadIdx.x, c = tid & 127, half = tid >> 7;
+  const int b = col0 + (c >> 1), part = c & 1;
   const bool valid = b < a.ncol;
-  const int JH = a.JH;
-
-  if (warp == 0) {
-    tc::tmem_alloc(&tslot, 512);
-    tc::tmem_relinquish();
-  }
-  if (tid == 0) {
-    tc::mbar_init(&mbar, 1);
-    tc::mbar_fence_init();
-  }
-  tc::fence_before();
-  __syncthreads();
-  tc::fence_after();
-  const uint32_t tbase = tslot;
-  uint32_t phase = 0;
-  bool ok = true;
-
-  // column exponents of the symmetric and antisymmetric halves
-  const double *col = reinterpret_cast<const double *>(a.F + ((long long)m * a.ncol + (valid ? b : 0)) * a.J) + part;
-  double mxs = 0.0, mxa = 0.0;
-  if (valid)
-    for (int jh = 0; jh < JH; ++jh) {
-      const double gn = col[2 * (JH + jh)], gs = col[2 * (JH - 1 - jh)];
-      mxs = fmax(mxs, fabs(gn + gs));
-      mxa = fmax(mxa, fabs(gn - gs));
-    }
-  int es = 0, ea = 0;
-  frexp(mxs, &es);
-  frexp(mxa, &ea);
-
-  for (int p = 0; p < 2 && ok; ++p) {
-    const int mp = m * 2 + p;
-    const int Rp = rows_of_parity(a.N, m, p);
-    const int np = a.tnpad[mp];
-    const int e = p ? ea : es;
-    const char *tab = reinterpret_cast<const char *>(a.tab + a.toff[mp]);
-    for (int kc = 0; kc < a.fwd_kch && ok; ++kc) {
-      // data digits of this thread's column into A (row = tid)
-      for (int kk = 0; kk < kKC; kk += 8) {
-        uint4 pk[kS];
-        unsigned short *pkh = reinterpret_cast<unsigned short *>(pk);
+  double m0 = 0.0, m1 = 0.0;
+  // loads are issued 8 at a time so that they are in flight together
+  if (!INV) {
+    // both parities of band m over all latitudes (done at the first chunk of (m, 0))
+    const double *col = reinterpret_cast<const double *>(a.F + ((long long)s.m * a.ncol + (valid ? b : 0)) * a.J) + part;
+    const int JH = a.JH, hh = (JH + 1) / 2;
+    const int j0 = half * hh, j1 = min(JH, (half + 1) * hh);
+    if (valid)
+      for (int jb = j0; jb < j1; jb += 8) {
+        double gn[8], gs[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          const int jh = kc * kKC + kk + q;
-          float d[kS];
-          double x = 0.0;
-          if (valid && jh < JH) {
-            const double gn = col[2 * (JH + jh)], gs = col[2 * (JH - 1 - jh)];
-            x = ldexp(p ? gn - gs : gn + gs, -e);
-          }
-          digits6(x, d);
-#pragma unroll
-          for (int s = 0; s < kS; ++s) pkh[s * 8 + q] = __bfloat16_as_ushort(__float2bfloat16_rn(d[s]));
+          const int jh = min(jb + q, j1 - 1);
+          gn[q] = col[2 * (JH + jh)];
+          gs[q] = col[2 * (JH - 1 - jh)];
         }
 #pragma unroll
-        for (int s = 0; s < kS; ++s)
-          *reinterpret_cast<uint4 *>(Asm + s * kM * kTileBytesPerRow + canon(tid, kk)) = pk[s];
-      }
-      // table digits for (m, p, chunk): kS tiles of np rows, contiguous
-      {
-        const uint4 *src = reinterpret_cast<const uint4 *>(tab + (size_t)kc * kS * np * kTileBytesPerRow);
-        uint4 *dst = reinterpret_cast<uint4 *>(Bsm);
-        const int n16 = kS * np * kTileBytesPerRow / 16;
-        for (int q = tid; q < n16; q += 128) dst[q] = src[q];
-      }
-      tc::fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) {
-        tc::fence_after();
-        issue_chunk(tbase, NPAD, tc::smem_addr(Asm), tc::smem_addr(Bsm), np, kc == 0);
-        tc::mma_commit(&mbar);
-      }
-      __syncwarp();
-      bool done = tc::mbar_wait(&mbar, phase, kWaitLimit);
-      if (!done && (tid & 31) == 0) atomicExch(a.err, SHT_ERR_DEVICE_TIMEOUT);
-      ok = __syncthreads_and(done) != 0;  // every thread takes the same path
-      if (ok) phase ^= 1;
-      tc::fence_after();
-    }
-    if (!ok) break;
-    // read the levels back: lane = this thread's column, columns = degrees of parity p
-    double acc[NPAD];
-#pragma unroll
-    for (int n = 0; n < NPAD; ++n) acc[n] = 0.0;
-    const uint32_t lane_base = tbase + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-    for (int L = kS - 1; L >= 0; --L) {
-#pragma unroll
-      for (int q = 0; q < NPAD / 16; ++q) {
-        uint32_t r[16];
-        tc::tmem_ld16(lane_base + (uint32_t)(L * NPAD + 16 * q), r);
-        tc::tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) acc[16 * q + i] = acc[16 * q + i] * (1.0 / 256.0) + (double)__uint_as_float(r[i]);
-      }
-    }
-    // acc = sum_L 2^{-8L} D_L; value = acc * 2^(e + f_n - 14)
-    if (valid) {
-      const int *fe = a.texp + a.teoff[mp];
-      const long long rowbase = a.rowoff[m];
-#pragma unroll
-      for (int n = 0; n < NPAD; ++n) {
-        if (n < Rp) {
-          const double v = ldexp(acc[n], e + fe[n] - 14);
-          reinterpret_cast<double *>(a.S + (rowbase + p + 2 * n) * a.ncol + b)[part] = v;
+        for (int q = 0; q < 8; ++q) {
+          m0 = fmax(m0, fabs(gn[q] + gs[q]));
+          m1 = fmax(m1, fabs(gn[q] - gs[q]));
         }
       }
-    }
-    tc::fence_before();  // TMEM reads above precede the next parity's MMAs
-    __syncthreads();
+  } else {
+    const double *cf = reinterpret_cast<const double *>(a.Sc + (long long)a.rowoff[s.m] * a.ncol + (valid ? b : 0)) + part;
+    const int hh = (s.Rp + 1) / 2;
+    const int i0 = half * hh, i1 = min(s.Rp, (half + 1) * hh);
+    if (valid)
+      for (int ib = i0; ib < i1; ib += 8) {
+        double v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) v[q] = cf[2 * (long long)(s.p + 2 * min(ib + q, i1 - 1)) * a.ncol];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) m0 = fmax(m0, fabs(v[q]));
+      }
   }
-  if (!ok) tc::mbar_wait(&mbar, phase, kWaitLimit);  // give in-flight MMAs a bounded chance to drain
-  tc::fence_before();
+  sm.part[(0 * 2 + half) * 128 + c] = m0;
+  sm.part[(1 * 2 + half) * 128 + c] = m1;
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tbase, 512);
+  if (half == 0) {
+    int e0 = 0, e1 = 0;
+    frexp(fmax(sm.part[0 * 128 + c], sm.part[1 * 128 + c]), &e0);
+    frexp(fmax(sm.part[2 * 128 + c], sm.part[3 * 128 + c]), &e1);
+    sm.exps[s.slot * 128 + c] = e0;
+    if (!INV) sm.exps[((s.slot + 1) & 3) * 128 + c] = e1;  // the (m, 1) sub-item follows in the next slot
+  }
+  __syncthreads();
 }
 
-// ----------------------------------------------------------------- synthesis
-template <int JHT>
-__global__ void __launch_bounds__(128, 1) k_leg_inv_split(TcArgs a)
+// Digits of chunk h of sub-item s into stage st (A), and the table chunk (B).
+template <bool INV>
+__device__ void prepare(const TcArgs &a, const Sub &s, int h, int col0, const Smem &sm, int st)
+{
+  const int tid = threadIdx.x;
+  const int JH = a.JH;
+  // A: 128 rows x 4 k-groups of 8; two tasks per thread
+  for (int task = tid; task < kM * (kKC / 8); task += kThreads) {
+    const int c = task & 127, kg = task >> 7;
+    const int b = col0 + (c >> 1), part = c & 1;
+    const bool valid = b < a.ncol;
+    const int e = sm.exps[s.slot * 128 + c];
+    uint4 pk[kS];
+    unsigned short *pkh = reinterpret_cast<unsigned short *>(pk);
+    if (!INV) {
+      const double *col = reinterpret_cast<const double *>(a.F + ((long long)s.m * a.ncol + (valid ? b : 0)) * a.J) + part;
+      const double sc = ldexp(1.0, -e);
+      double gn[8], gs[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int jh = min(h * kKC + kg * 8 + q, JH - 1);
+        gn[q] = valid ? col[2 * (JH + jh)] : 0.0;
+        gs[q] = valid ? col[2 * (JH - 1 - jh)] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int jh = h * kKC + kg * 8 + q;
+        double x = 0.0;
+        if (jh < JH) x = (s.p ? gn[q] - gs[q] : gn[q] + gs[q]) * sc;
+        unsigned short d[kS];
+        digits_bf16(x, d);
+#pragma unroll
+        for (int k = 0; k < kS; ++k) pkh[k * 8 + q] = d[k];
+      }
+    } else {
+      const double *cf = reinterpret_cast<const double *>(a.Sc + (long long)a.rowoff[s.m] * a.ncol + (valid ? b : 0)) + part;
+      const double sc = ldexp(1.0, -e);
+      double cv[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int i = min(h * kKC + kg * 8 + q, s.Rp - 1);
+        cv[q] = valid ? cf[2 * (long long)(s.p + 2 * i) * a.ncol] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int i = h * kKC + kg * 8 + q;
+        double x = 0.0;
+        if (i < s.Rp) x = cv[q] * sc;
+        unsigned short d[kS];
+        digits_bf16(x, d);
+#pragma unroll
+        for (int k = 0; k < kS; ++k) pkh[k * 8 + q] = d[k];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kS; ++k) *reinterpret_cast<uint4 *>(sm.A[st] + k * kM * kRowB + canon(c, kg * 8)) = pk[k];
+  }
+  // B: the table chunk (kS tiles of npad rows x 32 k), contiguous; copied
+  // asynchronously (all 16-byte pieces in flight at once), completed below
+  const int mp = s.m * 2 + s.p;
+  const char *src = reinterpret_cast<const char *>(a.tab + a.toff[mp]) + (size_t)h * kS * s.npad * kRowB;
+  const int n16 = kS * s.npad * kRowB / 16;
+  for (int q = tid; q < n16; q += kThreads)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(sm.B[st] + 16 * q)), "l"(src + 16 * q));
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+
+__device__ __forceinline__ void prepare_done() { asm volatile("cp.async.wait_group 0;\n" ::); }
+
+// Read the seven TMEM levels of sub-item s and write the results.
+template <bool INV>
+__device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm, uint32_t tbase)
+{
+  const int tid = threadIdx.x, warp = tid >> 5, c = tid & 127, half = tid >> 7;
+  const int b = col0 + (c >> 1), part = c & 1;
+  const bool valid = b < a.ncol;
+  const int e = sm.exps[s.slot * 128 + c];
+  const uint32_t lane_base = tbase + ((uint32_t)((warp & 3) * 32) << 16);
+  const int ngroups = s.npad / 16;
+  for (int g = half; g < ngroups; g += 2) {
+    double acc[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+#pragma unroll
+    for (int L = kS - 1; L >= 0; --L) {
+      uint32_t r[16];
+      tc::tmem_ld16(lane_base + (uint32_t)(L * a.npad_max + 16 * g), r);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i = 0; i < 16; ++i) acc[i] = acc[i] * (1.0 / 256.0) + (double)__uint_as_float(r[i]);
+    }
+    if (!valid) continue;
+    if (!INV) {
+      const int *fe = a.texp + a.teoff[s.m * 2 + s.p];
+      const long long rowbase = a.rowoff[s.m];
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int n = 16 * g + i;
+        if (n < s.Rp)
+          reinterpret_cast<double *>(a.S + (rowbase + s.p + 2 * n) * a.ncol + b)[part] = ldexp(acc[i], e + fe[n] - 14);
+      }
+    } else {
+      // The even half is parked in this thread's northern output slots and
+      // combined with the odd half on the second pass (same thread, same addresses).
+      const int *ge = a.texp + (s.m * 2 + s.p) * a.JH;
+      double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + b) * a.J) + part;
+      const int JH = a.JH;
+      double gev[16];
+      if (s.p == 1) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) gev[i] = (16 * g + i < JH) ? Fc[2 * (JH + 16 * g + i)] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int jh = 16 * g + i;
+        if (jh >= JH) continue;
+        const double v = ldexp(acc[i], e + ge[jh] - 14);
+        if (s.p == 0) {
+          Fc[2 * (JH + jh)] = v;
+        } else {
+          Fc[2 * (JH + jh)] = gev[i] + v;
+          Fc[2 * (JH - 1 - jh)] = gev[i] - v;
+        }
+      }
+    }
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(kThreads, 1) k_leg_split(TcArgs a)
 {
   extern __shared__ __align__(1024) unsigned char smem[];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar_stage[2], mbar_tmem;
   __shared__ uint32_t tslot;
-  unsigned char *Asm = smem;                               // kS x 128 x 64 bf16
-  unsigned char *Bsm = smem + kS * kM * kTileBytesPerRow;  // kS x JHT x 64 bf16
+  const int bstage = kS * a.npad_max * kRowB;
+  Smem sm;
+  sm.A[0] = smem;
+  sm.A[1] = smem + kS * kM * kRowB;
+  sm.B[0] = smem + 2 * kS * kM * kRowB;
+  sm.B[1] = sm.B[0] + bstage;
+  sm.exps = reinterpret_cast<int *>(sm.B[1] + bstage);
+  sm.part = reinterpret_cast<double *>(sm.exps + 4 * 128);
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int m = blockIdx.y, col0 = blockIdx.x * (kM / 2);
-  const int b = col0 + (tid >> 1), part = tid & 1;
-  const bool valid = b < a.ncol;
-  const int JH = a.JH;
+
+  const int it0 = blockIdx.x * a.per_cta;
+  const int it1 = min(a.nitems, it0 + a.per_cta);
+  if (it0 >= it1) return;
 
   if (warp == 0) {
     tc::tmem_alloc(&tslot, 512);
     tc::tmem_relinquish();
   }
   if (tid == 0) {
-    tc::mbar_init(&mbar, 1);
+    tc::mbar_init(&mbar_stage[0], 1);
+    tc::mbar_init(&mbar_stage[1], 1);
+    tc::mbar_init(&mbar_tmem, 1);
     tc::mbar_fence_init();
   }
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
   const uint32_t tbase = tslot;
-  uint32_t phase = 0;
+  uint32_t ph_stage[2] = {0, 0}, ph_tmem = 0;
   bool ok = true;
-  const long long rowbase = a.rowoff[m];
 
-  for (int p = 0; p < 2 && ok; ++p) {
-    const int mp = m * 2 + p;
-    const int Rp = rows_of_parity(a.N, m, p);
-    const int kch = (Rp + kKC - 1) / kKC;
-    // coefficient exponent of this column over the degrees of parity p
-    const double *cf = reinterpret_cast<const double *>(a.Sc + rowbase * a.ncol + (valid ? b : 0)) + part;
-    double mx = 0.0;
-    if (valid)
-      for (int i = 0; i < Rp; ++i) mx = fmax(mx, fabs(cf[2 * (long long)(p + 2 * i) * a.ncol]));
-    int e = 0;
-    frexp(mx, &e);
-    const char *tab = reinterpret_cast<const char *>(a.tab + a.toff[mp]);
-    for (int kc = 0; kc < kch && ok; ++kc) {
-      for (int kk = 0; kk < kKC; kk += 8) {
-        uint4 pk[kS];
-        unsigned short *pkh = reinterpret_cast<unsigned short *>(pk);
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int i = kc * kKC + kk + q;
-          float d[kS];
-          double x = 0.0;
-          if (valid && i < Rp) x = ldexp(cf[2 * (long long)(p + 2 * i) * a.ncol], -e);
-          digits6(x, d);
-#pragma unroll
-          for (int s = 0; s < kS; ++s) pkh[s * 8 + q] = __bfloat16_as_ushort(__float2bfloat16_rn(d[s]));
-        }
-#pragma unroll
-        for (int s = 0; s < kS; ++s)
-          *reinterpret_cast<uint4 *>(Asm + s * kM * kTileBytesPerRow + canon(tid, kk)) = pk[s];
-      }
-      {
-        const uint4 *src = reinterpret_cast<const uint4 *>(tab + (size_t)kc * kS * JHT * kTileBytesPerRow);
-        uint4 *dst = reinterpret_cast<uint4 *>(Bsm);
-        const int n16 = kS * JHT * kTileBytesPerRow / 16;
-        for (int q = tid; q < n16; q += 128) dst[q] = src[q];
-      }
-      tc::fence_proxy_async();
-      __syncthreads();
-      if (tid == 0) {
-        tc::fence_after();
-        issue_chunk(tbase, JHT, tc::smem_addr(Asm), tc::smem_addr(Bsm), JHT, kc == 0);
-        tc::mma_commit(&mbar);
-      }
-      __syncwarp();
-      bool done = tc::mbar_wait(&mbar, phase, kWaitLimit);
-      if (!done && (tid & 31) == 0) atomicExch(a.err, SHT_ERR_DEVICE_TIMEOUT);
-      ok = __syncthreads_and(done) != 0;  // every thread takes the same path
-      if (ok) phase ^= 1;
-      tc::fence_after();
-    }
-    if (!ok) break;
-    double acc[JHT];
-#pragma unroll
-    for (int n = 0; n < JHT; ++n) acc[n] = 0.0;
-    const uint32_t lane_base = tbase + ((uint32_t)(warp * 32) << 16);
-#pragma unroll
-    for (int L = kS - 1; L >= 0; --L) {
-#pragma unroll
-      for (int q = 0; q < JHT / 16; ++q) {
-        uint32_t r[16];
-        tc::tmem_ld16(lane_base + (uint32_t)(L * JHT + 16 * q), r);
-        tc::tmem_wait_ld();
-#pragma unroll
-        for (int i = 0; i < 16; ++i) acc[16 * q + i] = acc[16 * q + i] * (1.0 / 256.0) + (double)__uint_as_float(r[i]);
-      }
-    }
-    // The even half Ge is parked in this thread's northern output slots and
-    // combined with the odd half Go on the second pass (same thread, same addresses).
-    const int *ge = a.texp + mp * JH;
-    if (valid) {
-      double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)m * a.ncol + b) * a.J) + part;
-      if (p == 0) {
-#pragma unroll
-        for (int jh = 0; jh < JHT; ++jh)
-          if (jh < JH) Fc[2 * (JH + jh)] = ldexp(acc[jh], e + ge[jh] - 14);
-      } else {
-#pragma unroll
-        for (int jh = 0; jh < JHT; ++jh) {
-          if (jh < JH) {
-            const double go = ldexp(acc[jh], e + ge[jh] - 14), gev = Fc[2 * (JH + jh)];
-            Fc[2 * (JH + jh)] = gev + go;
-            Fc[2 * (JH - 1 - jh)] = gev - go;
-          }
-        }
-      }
-    }
-    tc::fence_before();  // TMEM reads above precede the next parity's MMAs
+  Cursor cur{it0, 0, 0, 0};
+  Sub s;
+  cursor_sub<INV>(a, cur, s);
+  {
+    const int col0 = (cur.it % a.ntiles) * (kM / 2);
+    column_exponents<INV>(a, s, col0, sm);
+    prepare<INV>(a, s, 0, col0, sm, 0);
+    prepare_done();
+    tc::fence_proxy_async();
     __syncthreads();
   }
-  if (!ok) tc::mbar_wait(&mbar, phase, kWaitLimit);  // give in-flight MMAs a bounded chance to drain
+  for (int u = 0;; ++u) {
+    const int st = u & 1;
+    const int col0 = (cur.it % a.ntiles) * (kM / 2);
+    cursor_sub<INV>(a, cur, s);
+    const bool last_chunk = (cur.h + 1 == s.nch);
+    if (tid == 0) {
+      tc::fence_after();
+      issue_chunk(tbase, a.npad_max, tc::smem_addr(sm.A[st]), tc::smem_addr(sm.B[st]), s.npad, cur.h == 0);
+      tc::mma_commit(&mbar_stage[st]);
+      if (last_chunk) tc::mma_commit(&mbar_tmem);
+    }
+    __syncwarp();
+    // prepare the next unit in the other stage while these MMAs run
+    Cursor nxt = cur;
+    cursor_next<INV>(a, nxt);
+    const bool more = nxt.it < it1;
+    if (more) {
+      Sub sn;
+      cursor_sub<INV>(a, nxt, sn);
+      const int ncol0 = (nxt.it % a.ntiles) * (kM / 2);
+      if (u >= 1) {  // the other stage is free once the MMAs of unit u-1 are done
+        const bool d = tc::mbar_wait(&mbar_stage[st ^ 1], ph_stage[st ^ 1], kWaitLimit);
+        if (!d && (tid & 31) == 0) atomicExch(a.err, SHT_ERR_DEVICE_TIMEOUT);
+        ok = __syncthreads_and(d) != 0;
+        ph_stage[st ^ 1] ^= 1;
+      }
+      if (ok) {
+        if (nxt.h == 0 && (INV || sn.p == 0)) column_exponents<INV>(a, sn, ncol0, sm);
+        prepare<INV>(a, sn, nxt.h, ncol0, sm, st ^ 1);
+        prepare_done();
+        tc::fence_proxy_async();
+      }
+    }
+    if (last_chunk && ok) {
+      const bool d = tc::mbar_wait(&mbar_tmem, ph_tmem, kWaitLimit);
+      if (!d && (tid & 31) == 0) atomicExch(a.err, SHT_ERR_DEVICE_TIMEOUT);
+      ok = __syncthreads_and(d) != 0;
+      ph_tmem ^= 1;
+      tc::fence_after();
+      if (ok) readout<INV>(a, s, col0, sm, tbase);
+      tc::fence_before();
+    }
+    ok = __syncthreads_and(ok) != 0;
+    if (!more || !ok) break;
+    cur = nxt;
+  }
+  if (!ok) tc::mbar_wait(&mbar_tmem, ph_tmem, kWaitLimit);  // give in-flight MMAs a bounded chance to drain
   tc::fence_before();
   __syncthreads();
   if (warp == 0) tc::tmem_dealloc(tbase, 512);
@@ -440,31 +548,29 @@ int build_split_tables(sht_plan *p)
   if (p->tc_tables) return SHT_OK;
   const int N = p->N, JH = p->JH;
   auto *t = new SplitTables();
-  // analysis table sizes
   std::vector<long long> foff(2 * (N + 1)), ioff(2 * (N + 1));
-  std::vector<int> feoff(2 * (N + 1)), fnpad(2 * (N + 1));
-  const int fkch = (JH + kKC - 1) / kKC;
-  long long fsz = 0, isz = 0;
-  int erows = 0, npmax = 0;
+  std::vector<int> feoff(2 * (N + 1));
+  const int fch = (JH + kKC - 1) / kKC;
   const int inpad = round_up(JH, 16);
+  long long fsz = 0, isz = 0;
+  int erows = 0, npmax = 16;
   for (int m = 0; m <= N; ++m)
     for (int pp = 0; pp < 2; ++pp) {
       const int mp = 2 * m + pp, Rp = rows_of_parity(N, m, pp);
       const int np = round_up(Rp > 0 ? Rp : 1, 16);
-      fnpad[mp] = np;
       npmax = np > npmax ? np : npmax;
       foff[mp] = fsz;
-      fsz += (long long)fkch * kS * np * kKC;
+      fsz += (long long)fch * kS * np * kKC;
       feoff[mp] = erows;
       erows += Rp;
       ioff[mp] = isz;
       isz += (long long)((Rp + kKC - 1) / kKC) * kS * inpad * kKC;
     }
-  t->npad_max = npmax;
-  t->fwd_kch = fkch;
+  t->fwd_npad_max = npmax;
+  t->inv_npad = inpad;
   cudaError_t e;
   auto fail = [&](cudaError_t err, const char *what) {
-    cudaFree(t->fwd); cudaFree(t->fwd_off); cudaFree(t->fwd_exp); cudaFree(t->fwd_eoff); cudaFree(t->fwd_npad);
+    cudaFree(t->fwd); cudaFree(t->fwd_off); cudaFree(t->fwd_exp); cudaFree(t->fwd_eoff);
     cudaFree(t->inv); cudaFree(t->inv_off); cudaFree(t->inv_exp); cudaFree(t->d_err);
     delete t;
     return cuda_fail(err, what);
@@ -474,7 +580,6 @@ int build_split_tables(sht_plan *p)
   if ((e = cudaMalloc(&t->fwd_off, sizeof(long long) * foff.size())) != cudaSuccess) return fail(e, "split table");
   if ((e = cudaMalloc(&t->inv_off, sizeof(long long) * ioff.size())) != cudaSuccess) return fail(e, "split table");
   if ((e = cudaMalloc(&t->fwd_eoff, sizeof(int) * feoff.size())) != cudaSuccess) return fail(e, "split table");
-  if ((e = cudaMalloc(&t->fwd_npad, sizeof(int) * fnpad.size())) != cudaSuccess) return fail(e, "split table");
   if ((e = cudaMalloc(&t->fwd_exp, sizeof(int) * (erows > 0 ? erows : 1))) != cudaSuccess) return fail(e, "split table");
   if ((e = cudaMalloc(&t->inv_exp, sizeof(int) * 2 * (N + 1) * JH)) != cudaSuccess) return fail(e, "split table");
   if ((e = cudaMalloc(&t->d_err, sizeof(int))) != cudaSuccess) return fail(e, "split table");
@@ -484,12 +589,11 @@ int build_split_tables(sht_plan *p)
       (e = cudaMemsetAsync(t->d_err, 0, sizeof(int), s)) != cudaSuccess ||
       (e = cudaMemcpyAsync(t->fwd_off, foff.data(), sizeof(long long) * foff.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
       (e = cudaMemcpyAsync(t->inv_off, ioff.data(), sizeof(long long) * ioff.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(t->fwd_eoff, feoff.data(), sizeof(int) * feoff.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(t->fwd_npad, fnpad.data(), sizeof(int) * fnpad.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      (e = cudaMemcpyAsync(t->fwd_eoff, feoff.data(), sizeof(int) * feoff.size(), cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return fail(e, "split table upload");
   const int maxrows = (N + 3) / 2;
   dim3 gf((maxrows + 127) / 128, 2 * (N + 1));
-  k_slice_table_fwd<<<gf, 128, 0, s>>>(N, JH, p->d_P, p->d_poff, t->fwd, t->fwd_off, t->fwd_exp, t->fwd_eoff, t->fwd_npad, fkch);
+  k_slice_table_fwd<<<gf, 128, 0, s>>>(N, JH, p->d_P, p->d_poff, t->fwd, t->fwd_off, t->fwd_exp, t->fwd_eoff);
   count_launch();
   dim3 gi((JH + 127) / 128, 2 * (N + 1));
   k_slice_table_inv<<<gi, 128, 0, s>>>(N, JH, p->d_P, p->d_poff, t->inv, t->inv_off, t->inv_exp, inpad);
@@ -499,75 +603,65 @@ int build_split_tables(sht_plan *p)
   return SHT_OK;
 }
 
-size_t fwd_smem(int npad) { return (size_t)kS * kM * kTileBytesPerRow + (size_t)kS * npad * kTileBytesPerRow; }
-size_t inv_smem(int jht) { return (size_t)kS * kM * kTileBytesPerRow + (size_t)kS * jht * kTileBytesPerRow; }
-
-template <typename K>
-int launch_tc(K kern, dim3 grid, size_t smem, cudaStream_t s, const TcArgs &a, const char *name)
+size_t split_smem(int npad_max)
 {
+  return 2 * (size_t)kS * kM * kRowB + 2 * (size_t)kS * npad_max * kRowB + 4 * 128 * sizeof(int) + 4 * 128 * sizeof(double);
+}
+
+int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2 *out, cudaStream_t s)
+{
+  if (ncol <= 0) return SHT_OK;
+  if (!split_supported(p)) {
+    set_error("split precision: this grid is not covered by the tensor-core kernel "
+              "(needs jm <= 128 with jm/2 a multiple of 16, and nm <= 125)");
+    return SHT_ERR_UNSUPPORTED_SIZE;
+  }
+  int rc = build_split_tables(p);
+  if (rc) return rc;
+  SplitTables *t = tables(p);
+  TcArgs a{};
+  if (inverse) {
+    a.Sc = in; a.Fo = out; a.tab = t->inv; a.toff = t->inv_off; a.texp = t->inv_exp; a.npad_max = t->inv_npad;
+  } else {
+    a.F = in; a.S = out; a.tab = t->fwd; a.toff = t->fwd_off; a.texp = t->fwd_exp; a.teoff = t->fwd_eoff;
+    a.npad_max = t->fwd_npad_max;
+  }
+  a.rowoff = p->d_rowoff; a.pairs = p->d_pairs;
+  a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol; a.err = t->d_err;
+  a.ntiles = (ncol + kM / 2 - 1) / (kM / 2);
+  a.nitems = p->n_pairs * a.ntiles;
+  const int slots = p->num_sms;
+  a.per_cta = (a.nitems + slots - 1) / slots;
+  const int grid = (a.nitems + a.per_cta - 1) / a.per_cta;
+  const size_t smem = split_smem(a.npad_max);
+  auto kern = inverse ? k_leg_split<true> : k_leg_split<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, name);
-  kern<<<grid, 128, smem, s>>>(a);
+  if (e != cudaSuccess) return cuda_fail(e, "split smem attribute");
+  kern<<<grid, kThreads, smem, s>>>(a);
   count_launch();
   e = cudaGetLastError();
-  return e == cudaSuccess ? SHT_OK : cuda_fail(e, name);
+  return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_leg_split<inv>" : "k_leg_split<fwd>");
 }
 
 }  // namespace
 
 bool split_supported(const sht_plan *p)
 {
-  // TMEM holds the kS levels of one parity: kS * NPAD <= 512 columns.
+  // TMEM holds the kS levels of one sub-item: kS * NPAD <= 512 columns; the
+  // accumulation over at most 128 latitudes or degrees keeps every level exact.
   const int npmax = round_up((p->N + 3) / 2, 16);
-  return p->JH <= kKC && (p->JH % 16) == 0 && npmax * kS <= 512 && p->JH * kS <= 512;
+  const int inpad = round_up(p->JH, 16);
+  return p->JH <= 64 && npmax * kS <= 512 && inpad * kS <= 512 && split_smem(npmax > inpad ? npmax : inpad) <= 227 * 1024;
 }
 
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
 {
-  if (ncol <= 0) return SHT_OK;
-  if (!split_supported(p)) {
-    set_error("split precision: this grid is not covered by the tensor-core kernel (needs jm <= 128 with jm/2 a multiple of 16, nm <= 125)");
-    return SHT_ERR_UNSUPPORTED_SIZE;
-  }
-  int rc = build_split_tables(p);
-  if (rc) return rc;
-  SplitTables *t = tables(p);
-  TcArgs a{};
-  a.F = F; a.S = S; a.rowoff = p->d_rowoff; a.tab = t->fwd; a.toff = t->fwd_off; a.texp = t->fwd_exp;
-  a.teoff = t->fwd_eoff; a.tnpad = t->fwd_npad; a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;
-  a.fwd_kch = t->fwd_kch; a.err = t->d_err;
-  dim3 grid((ncol + kM / 2 - 1) / (kM / 2), p->N + 1);
-  const int np = t->npad_max;
-  switch (np) {
-  case 16: return launch_tc(k_leg_fwd_split<16>, grid, fwd_smem(16), s, a, "k_leg_fwd_split");
-  case 32: return launch_tc(k_leg_fwd_split<32>, grid, fwd_smem(32), s, a, "k_leg_fwd_split");
-  case 48: return launch_tc(k_leg_fwd_split<48>, grid, fwd_smem(48), s, a, "k_leg_fwd_split");
-  case 64: return launch_tc(k_leg_fwd_split<64>, grid, fwd_smem(64), s, a, "k_leg_fwd_split");
-  default: set_error("split precision: unsupported row count"); return SHT_ERR_UNSUPPORTED_SIZE;
-  }
+  return launch_split(p, false, F, ncol, S, s);
 }
 
 int launch_leg_inv_split(sht_plan *p, const double2 *Sp, int ncol, double2 *F, cudaStream_t s)
 {
-  if (ncol <= 0) return SHT_OK;
-  if (!split_supported(p)) {
-    set_error("split precision: this grid is not covered by the tensor-core kernel (needs jm <= 128 with jm/2 a multiple of 16, nm <= 125)");
-    return SHT_ERR_UNSUPPORTED_SIZE;
-  }
-  int rc = build_split_tables(p);
-  if (rc) return rc;
-  SplitTables *t = tables(p);
-  TcArgs a{};
-  a.Sc = Sp; a.Fo = F; a.rowoff = p->d_rowoff; a.tab = t->inv; a.toff = t->inv_off; a.texp = t->inv_exp;
-  a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol; a.err = t->d_err;
-  dim3 grid((ncol + kM / 2 - 1) / (kM / 2), p->N + 1);
-  switch (p->JH) {
-  case 16: return launch_tc(k_leg_inv_split<16>, grid, inv_smem(16), s, a, "k_leg_inv_split");
-  case 32: return launch_tc(k_leg_inv_split<32>, grid, inv_smem(32), s, a, "k_leg_inv_split");
-  case 48: return launch_tc(k_leg_inv_split<48>, grid, inv_smem(48), s, a, "k_leg_inv_split");
-  case 64: return launch_tc(k_leg_inv_split<64>, grid, inv_smem(64), s, a, "k_leg_inv_split");
-  default: set_error("split precision: unsupported latitude count"); return SHT_ERR_UNSUPPORTED_SIZE;
-  }
+  return launch_split(p, true, Sp, ncol, F, s);
 }
 
 int split_error_status(sht_plan *p)
@@ -589,7 +683,7 @@ void free_split_tables(sht_plan *p)
 {
   SplitTables *t = tables(p);
   if (!t) return;
-  cudaFree(t->fwd); cudaFree(t->fwd_off); cudaFree(t->fwd_exp); cudaFree(t->fwd_eoff); cudaFree(t->fwd_npad);
+  cudaFree(t->fwd); cudaFree(t->fwd_off); cudaFree(t->fwd_exp); cudaFree(t->fwd_eoff);
   cudaFree(t->inv); cudaFree(t->inv_off); cudaFree(t->inv_exp); cudaFree(t->d_err);
   delete t;
   p->tc_tables = nullptr;
