@@ -76,6 +76,8 @@ __device__ __forceinline__ void dft_reg(double2 (&v)[1 << LOG])
         const int t = k * (32 / (2 * h));  // W_{2h}^k = exp(-+ 2 pi i t / 32)
         if (t == 0) {
           v[b + k + h] = make_double2(dx, dy);
+        } else if (t == 8) {  // W = -+i
+          v[b + k + h] = INV ? make_double2(-dy, dx) : make_double2(dy, -dx);
         } else {
           const double wr = cos32(t);
           const double wi = INV ? sin32(t) : -sin32(t);
@@ -117,210 +119,305 @@ struct FftArgs {
   int I, J, N;
 };
 
+// Shared-memory plan of one thread block: the twiddle tables (2 NC entries),
+// then two buffers, each large enough for a staged input tile and, in place,
+// for every later stage of that tile.
 template <int A, int B, int NT>
-__global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
+struct FftShape {
+  static constexpr int R1 = 1 << A, R2 = 1 << B, NC = R1 * R2, T = R2, JT = NT / T;
+  static constexpr int RS = fft_row_stride<R1, R2, T>();
+  static constexpr int JTp = fft_out_stride(JT, T);
+  // staged grid rows are padded so that the 8/T rows of one 8-lane phase of a
+  // 16-byte access fall into distinct bank groups
+  static constexpr int NCp = NC + (T < 8 ? T : 0);
+  static int buf_elems(int N)  // double2 per buffer
+  {
+    int b = JT * NCp;
+    b = b > JT * RS ? b : JT * RS;
+    b = b > (N + 1) * JTp ? b : (N + 1) * JTp;
+    return (b + 7) & ~7;
+  }
+};
+
+__device__ __forceinline__ void cp_async16(void *dst_smem, const void *src, bool fill)
 {
-  constexpr int R1 = 1 << A, R2 = 1 << B, NC = R1 * R2, T = R2, JT = NT / T;
-  constexpr int RS = fft_row_stride<R1, R2, T>();
-  constexpr int JTp = fft_out_stride(JT, T);
-  constexpr int NS = R1 / T;
-  extern __shared__ double2 sm[];
+  // src-size 0 writes 16 zero bytes and reads nothing
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"((uint32_t)__cvta_generic_to_shared(dst_smem)),
+               "l"(src), "r"(fill ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
 
-  const int tid = threadIdx.x, r = tid / T, u = tid % T;
-  const int ntile = (a.J + JT - 1) / JT;
-  const int col = blockIdx.x / ntile, jt = blockIdx.x - col * ntile;
-  const int j0 = jt * JT, j = j0 + r;
-  const bool valid = j < a.J;
-  const long long IJ = (long long)a.I * a.J;
-  const double *src = (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
-
-  // pass A: R1-point DFTs over elements strided by R2
-  double2 v[R1];
-  if (valid) {
-    const double2 *rowp = reinterpret_cast<const double2 *>(src + (long long)j * a.I);
-#pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) v[n1] = __ldcs(rowp + R2 * n1 + u);
-  } else {
-#pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) v[n1] = make_double2(0.0, 0.0);
+// Both twiddle tables go to shared memory once per block (L1 keeps little
+// room next to the staging buffers): stw[k1 T + u] = e^{-2 pi i u k1 / NC}
+// for the four-step twiddle of thread column u, stwI[m] = e^{-2 pi i m / I}.
+// The first barrier of the tile loop publishes them.
+template <int T, int NC, int NT>
+__device__ __forceinline__ void load_twiddles(const FftArgs &a, double2 *stw, double2 *stwI)
+{
+  for (int q = threadIdx.x; q < NC; q += NT) {
+    stw[q] = __ldg(a.tw + (q % T) * (q / T));
+    stwI[q] = __ldg(a.twI + q);
   }
-  dft_reg<A, false>(v);
-  double2 *srow = sm + r * RS;
-#pragma unroll
-  for (int k1 = 0; k1 < R1; ++k1) {
-    double2 y = v[brev<A>(k1)];
-    if (k1 != 0) y = cmul(y, __ldg(a.tw + u * k1));
-    srow[u * (R1 + 1) + k1] = y;
-  }
-  __syncthreads();
-
-  // pass B: R2-point DFTs
-  double2 z[NS][R2];
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const int k1 = u + T * s;
-#pragma unroll
-    for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
-    dft_reg<B, false>(z[s]);
-  }
-  __syncthreads();
-#pragma unroll
-  for (int s = 0; s < NS; ++s)
-#pragma unroll
-    for (int k2 = 0; k2 < R2; ++k2) srow[(u + T * s) + R1 * k2] = z[s][brev<B>(k2)];
-  __syncthreads();
-
-  // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I}
-  const double sc = valid ? __ldg(a.rowscale + j) : 0.0;
-  double2 xo[R1];
-#pragma unroll
-  for (int q = 0; q < R1; ++q) {
-    const int m = u + T * q;
-    xo[q] = make_double2(0.0, 0.0);
-    if (m <= a.N) {
-      const int mm = (NC - m) & (NC - 1);
-      const double2 zm = srow[m], zc = srow[mm];
-      const double er = 0.5 * (zm.x + zc.x), ei = 0.5 * (zm.y - zc.y);
-      const double dr = 0.5 * (zm.x - zc.x), di = 0.5 * (zm.y + zc.y);
-      const double2 w = __ldg(a.twI + m);
-      const double tr = w.x * dr - w.y * di, ti = w.x * di + w.y * dr;
-      xo[q] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
-    }
-  }
-  __syncthreads();
-#pragma unroll
-  for (int q = 0; q < R1; ++q) {
-    const int m = u + T * q;
-    if (m <= a.N) sm[m * JTp + r] = xo[q];
-  }
-  __syncthreads();
-
-  const int nrows = min(JT, a.J - j0);
-  const int total = (a.N + 1) * JT;
-  double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + j0;
-  const long long mstride = (long long)a.ncolF * a.J;
-  for (int idx = tid; idx < total; idx += NT) {
-    const int m = idx / JT, rr = idx - m * JT;
-    if (rr < nrows) Fb[m * mstride + rr] = sm[m * JTp + rr];
-  }
-  (void)NC;
 }
 
+// Forward transform, persistent over tiles (field-level, JT latitude rows).
+// Tile t+gridDim.x streams into one buffer (cp.async, 16 bytes per thread per
+// copy) while tile t is transformed in place in the other.
 template <int A, int B, int NT>
-__global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a)
+__global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
 {
-  constexpr int R1 = 1 << A, R2 = 1 << B, NC = R1 * R2, T = R2, JT = NT / T;
-  constexpr int RS = fft_row_stride<R1, R2, T>();
-  constexpr int JTp = fft_out_stride(JT, T);
+  using S = FftShape<A, B, NT>;
+  constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT, RS = S::RS, JTp = S::JTp, NCp = S::NCp;
   constexpr int NS = R1 / T;
-  extern __shared__ double2 sm[];
+  extern __shared__ __align__(16) double2 smem_all[];
+  double2 *stw = smem_all, *stwI = smem_all + NC, *sm = smem_all + 2 * NC;
+  load_twiddles<T, NC, NT>(a, stw, stwI);
 
   const int tid = threadIdx.x, r = tid / T, u = tid % T;
   const int ntile = (a.J + JT - 1) / JT;
-  const int col = blockIdx.x / ntile, jt = blockIdx.x - col * ntile;
-  const int j0 = jt * JT, j = j0 + r;
-  const bool valid = j < a.J;
-  const int nrows = min(JT, a.J - j0);
-
-  // stage G^m for the tile's rows
-  const double2 *Fb = a.Fc + (long long)(a.colF0 + col) * a.J + j0;
+  const long long ntot = (long long)a.ncol * ntile;
+  const long long IJ = (long long)a.I * a.J;
   const long long mstride = (long long)a.ncolF * a.J;
-  for (int idx = tid; idx < (a.N + 1) * JT; idx += NT) {
-    const int m = idx / JT, rr = idx - m * JT;
-    sm[m * JTp + rr] = (rr < nrows) ? Fb[m * mstride + rr] : make_double2(0.0, 0.0);
-  }
-  __syncthreads();
 
-  // real pack: Z_k = (X_k + Y_k) + i w^k (X_k - Y_k), Y_k = conj X_{NC-k}, w = e^{+2 pi i/I}
-  double2 v[R1];
-#pragma unroll
-  for (int n1 = 0; n1 < R1; ++n1) {
-    const int k = R2 * n1 + u;
-    double2 X = make_double2(0.0, 0.0), Y = make_double2(0.0, 0.0);
-    if (k <= a.N) {
-      X = sm[k * JTp + r];
-      if (k == 0) X.y = 0.0;
+  auto issue = [&](long long t, double2 *buf) {
+    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT;
+    const double2 *src = reinterpret_cast<const double2 *>(
+        ((col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ) + (long long)j0 * a.I);
+    const int nrows = min(JT, a.J - j0);
+#pragma unroll 4
+    for (int q = tid; q < JT * NC; q += NT) {
+      const int rr = q / NC, c = q - rr * NC;
+      if (rr < nrows) cp_async16(buf + rr * NCp + c, src + (long long)rr * NC + c, true);
     }
-    const int kk = NC - k;
-    if (k > 0 && kk <= a.N) {
-      const double2 t = sm[kk * JTp + r];
-      Y = make_double2(t.x, -t.y);
+  };
+
+  long long t = blockIdx.x;
+  if (t < ntot) issue(t, sm);
+  cp_async_commit();
+  for (int it = 0; t < ntot; t += gridDim.x, ++it) {
+    double2 *cur = sm + (it & 1) * bufe;
+    if (t + gridDim.x < ntot) issue(t + gridDim.x, sm + ((it + 1) & 1) * bufe);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+
+    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT, j = j0 + r;
+    const bool valid = j < a.J;
+    // pass A: R1-point DFTs over elements strided by R2
+    double2 v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? cur[r * NCp + R2 * n1 + u] : make_double2(0.0, 0.0);
+    __syncthreads();  // the staged tile is consumed; the buffer is reused below
+    dft_reg<A, false>(v);
+    double2 *srow = cur + r * RS;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      double2 y = v[brev<A>(k1)];
+      if (k1 != 0) y = cmul(y, stw[k1 * T + u]);
+      srow[u * (R1 + 1) + k1] = y;
     }
-    const double2 wI = __ldg(a.twI + k);
-    const double wr = wI.x, wi = -wI.y;
-    const double dr = X.x - Y.x, di = X.y - Y.y;
-    const double tr = wr * dr - wi * di, ti = wr * di + wi * dr;
-    v[n1] = make_double2((X.x + Y.x) - ti, (X.y + Y.y) + tr);
-  }
-  __syncthreads();
+    __syncthreads();
 
-  dft_reg<A, true>(v);
-  double2 *srow = sm + r * RS;
+    // pass B: R2-point DFTs
+    double2 z[NS][R2];
 #pragma unroll
-  for (int k1 = 0; k1 < R1; ++k1) {
-    double2 y = v[brev<A>(k1)];
-    if (k1 != 0) y = cmulc(y, __ldg(a.tw + u * k1));
-    srow[u * (R1 + 1) + k1] = y;
-  }
-  __syncthreads();
-
-  double2 z[NS][R2];
+    for (int s = 0; s < NS; ++s) {
+      const int k1 = u + T * s;
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const int k1 = u + T * s;
-#pragma unroll
-    for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
-    dft_reg<B, true>(z[s]);
-  }
-  if (valid) {
-    const long long IJ = (long long)a.I * a.J;
-    double *dst = (col < a.nsplit) ? a.o0 + (long long)col * IJ : a.o1 + (long long)(col - a.nsplit) * IJ;
-    double2 *rowp = reinterpret_cast<double2 *>(dst + (long long)j * a.I);
-    const double sc = __ldg(a.rowscale + j);
+      for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
+      dft_reg<B, false>(z[s]);
+    }
+    __syncthreads();
 #pragma unroll
     for (int s = 0; s < NS; ++s)
 #pragma unroll
-      for (int k2 = 0; k2 < R2; ++k2) {
-        const double2 w = z[s][brev<B>(k2)];
-        __stcs(rowp + (u + T * s + R1 * k2), make_double2(w.x * sc, w.y * sc));
+      for (int k2 = 0; k2 < R2; ++k2) srow[(u + T * s) + R1 * k2] = z[s][brev<B>(k2)];
+    __syncthreads();
+
+    // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I}
+    const double sc = valid ? __ldg(a.rowscale + j) : 0.0;
+    double2 xo[R1];
+#pragma unroll
+    for (int q = 0; q < R1; ++q) {
+      const int m = u + T * q;
+      xo[q] = make_double2(0.0, 0.0);
+      if (m <= a.N) {
+        const int mm = (NC - m) & (NC - 1);
+        const double2 zm = srow[m], zc = srow[mm];
+        const double er = 0.5 * (zm.x + zc.x), ei = 0.5 * (zm.y - zc.y);
+        const double dr = 0.5 * (zm.x - zc.x), di = 0.5 * (zm.y + zc.y);
+        const double2 w = stwI[m];
+        const double tr = w.x * dr - w.y * di, ti = w.x * di + w.y * dr;
+        xo[q] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
       }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < R1; ++q) {
+      const int m = u + T * q;
+      if (m <= a.N) cur[m * JTp + r] = xo[q];
+    }
+    __syncthreads();
+
+    // Fourier runs F[m][col][j0 .. j0+JT)
+    const int nrows = min(JT, a.J - j0);
+    double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + j0;
+    for (int idx = tid; idx < (a.N + 1) * JT; idx += NT) {
+      const int m = idx / JT, rr = idx - m * JT;
+      if (rr < nrows) Fb[m * mstride + rr] = cur[m * JTp + rr];
+    }
+    __syncthreads();  // the buffer is refilled by the prefetch of the next iteration
   }
-  (void)NC;
+  cp_async_wait<0>();
+}
+
+// Inverse transform, persistent over tiles; the Fourier runs of tile
+// t+gridDim.x stream into one buffer while tile t is transformed in place.
+template <int A, int B, int NT>
+__global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
+{
+  using S = FftShape<A, B, NT>;
+  constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT, RS = S::RS, JTp = S::JTp;
+  constexpr int NS = R1 / T;
+  extern __shared__ __align__(16) double2 smem_all[];
+  double2 *stw = smem_all, *stwI = smem_all + NC, *sm = smem_all + 2 * NC;
+  load_twiddles<T, NC, NT>(a, stw, stwI);
+
+  const int tid = threadIdx.x, r = tid / T, u = tid % T;
+  const int ntile = (a.J + JT - 1) / JT;
+  const long long ntot = (long long)a.ncol * ntile;
+  const long long mstride = (long long)a.ncolF * a.J;
+
+  auto issue = [&](long long t, double2 *buf) {
+    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT;
+    const double2 *Fb = a.Fc + (long long)(a.colF0 + col) * a.J + j0;
+    const int nrows = min(JT, a.J - j0);
+    for (int idx = tid; idx < (a.N + 1) * JT; idx += NT) {
+      const int m = idx / JT, rr = idx - m * JT;
+      const bool in = rr < nrows;
+      cp_async16(buf + m * JTp + rr, in ? Fb + m * mstride + rr : Fb, in);
+    }
+  };
+
+  long long t = blockIdx.x;
+  if (t < ntot) issue(t, sm);
+  cp_async_commit();
+  for (int it = 0; t < ntot; t += gridDim.x, ++it) {
+    double2 *cur = sm + (it & 1) * bufe;
+    if (t + gridDim.x < ntot) issue(t + gridDim.x, sm + ((it + 1) & 1) * bufe);
+    cp_async_commit();
+    cp_async_wait<1>();
+    __syncthreads();
+
+    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT, j = j0 + r;
+    const bool valid = j < a.J;
+
+    // real pack: Z_k = (X_k + Y_k) + i w^k (X_k - Y_k), Y_k = conj X_{NC-k}, w = e^{+2 pi i/I}
+    double2 v[R1];
+#pragma unroll
+    for (int n1 = 0; n1 < R1; ++n1) {
+      const int k = R2 * n1 + u;
+      double2 X = make_double2(0.0, 0.0), Y = make_double2(0.0, 0.0);
+      if (k <= a.N) {
+        X = cur[k * JTp + r];
+        if (k == 0) X.y = 0.0;
+      }
+      const int kk = NC - k;
+      if (k > 0 && kk <= a.N) {
+        const double2 q = cur[kk * JTp + r];
+        Y = make_double2(q.x, -q.y);
+      }
+      const double2 wI = stwI[k];
+      const double wr = wI.x, wi = -wI.y;
+      const double dr = X.x - Y.x, di = X.y - Y.y;
+      const double tr = wr * dr - wi * di, ti = wr * di + wi * dr;
+      v[n1] = make_double2((X.x + Y.x) - ti, (X.y + Y.y) + tr);
+    }
+    __syncthreads();  // the staged runs are consumed; the buffer is reused below
+
+    dft_reg<A, true>(v);
+    double2 *srow = cur + r * RS;
+#pragma unroll
+    for (int k1 = 0; k1 < R1; ++k1) {
+      double2 y = v[brev<A>(k1)];
+      if (k1 != 0) y = cmulc(y, stw[k1 * T + u]);
+      srow[u * (R1 + 1) + k1] = y;
+    }
+    __syncthreads();
+
+    double2 z[NS][R2];
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const int k1 = u + T * s;
+#pragma unroll
+      for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
+      dft_reg<B, true>(z[s]);
+    }
+    if (valid) {
+      const long long IJ = (long long)a.I * a.J;
+      double *dst = (col < a.nsplit) ? a.o0 + (long long)col * IJ : a.o1 + (long long)(col - a.nsplit) * IJ;
+      double2 *rowp = reinterpret_cast<double2 *>(dst + (long long)j * a.I);
+      const double sc = __ldg(a.rowscale + j);
+#pragma unroll
+      for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int k2 = 0; k2 < R2; ++k2) {
+          const double2 w = z[s][brev<B>(k2)];
+          __stcs(rowp + (u + T * s + R1 * k2), make_double2(w.x * sc, w.y * sc));
+        }
+    }
+    __syncthreads();  // the buffer is refilled by the prefetch of the next iteration
+  }
+  cp_async_wait<0>();
 }
 
 namespace {
 constexpr int kFftThreads = 128;
 
-template <int A, int B>
-size_t fft_smem_bytes(int N)
+// Persistent grid: as many blocks as fit on the device at once, never more
+// than there are tiles.  The occupancy query runs once per kernel instance and
+// buffer size.
+template <typename K>
+int persistent_blocks(K kern, size_t smem, const sht_plan *p, long long ntiles)
 {
-  constexpr int R1 = 1 << A, R2 = 1 << B, T = R2, JT = kFftThreads / T;
-  constexpr int RS = fft_row_stride<R1, R2, T>();
-  const size_t s1 = (size_t)JT * RS;
-  const size_t s2 = (size_t)(N + 1) * fft_out_stride(JT, T);
-  return sizeof(double2) * (s1 > s2 ? s1 : s2);
+  struct Entry { const void *k; size_t smem; int occ; };
+  static std::mutex mu;
+  static std::vector<Entry> cache;
+  int occ = 0;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    for (const Entry &c : cache)
+      if (c.k == (const void *)kern && c.smem == smem) occ = c.occ;
+  }
+  if (occ == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreads, smem) != cudaSuccess || occ < 1) occ = 1;
+    std::lock_guard<std::mutex> lk(mu);
+    cache.push_back({(const void *)kern, smem, occ});
+  }
+  const long long g = (long long)occ * (p->num_sms > 0 ? p->num_sms : 1);
+  return (int)(ntiles < g ? ntiles : g);
 }
 
 template <int A, int B>
 int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s)
 {
-  constexpr int T = 1 << B, JT = kFftThreads / T;
-  const size_t smem = fft_smem_bytes<A, B>(p->N);
-  const long long nblk = (long long)args.ncol * ((p->J + JT - 1) / JT);
-  if (nblk <= 0) return SHT_OK;
-  if (nblk > 0x7fffffffLL) { set_error("fft: too many columns"); return SHT_ERR_TOO_LARGE; }
-  cudaError_t e;
-  if (inverse) {
-    auto kern = k_fft_inv<A, B, kFftThreads>;
-    if (smem > 48 * 1024 && (e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-      return cuda_fail(e, "fft_inv smem attribute");
-    kern<<<(unsigned)nblk, kFftThreads, smem, s>>>(args);
-  } else {
-    auto kern = k_fft_fwd<A, B, kFftThreads>;
-    if (smem > 48 * 1024 && (e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-      return cuda_fail(e, "fft_fwd smem attribute");
-    kern<<<(unsigned)nblk, kFftThreads, smem, s>>>(args);
-  }
+  using S = FftShape<A, B, kFftThreads>;
+  const int bufe = S::buf_elems(p->N);
+  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)bufe);
+  const long long ntiles = (long long)args.ncol * ((p->J + S::JT - 1) / S::JT);
+  if (ntiles <= 0) return SHT_OK;
+  if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
+  cudaError_t e = cudaSuccess;
+  auto go = [&](auto kern) {
+    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return;
+    kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(args, bufe);
+  };
+  if (inverse) go(k_fft_inv<A, B, kFftThreads>);
+  else go(k_fft_fwd<A, B, kFftThreads>);
+  if (e != cudaSuccess) return cuda_fail(e, "fft smem attribute");
   count_launch();
   e = cudaGetLastError();
   return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_fft_inv" : "k_fft_fwd");

@@ -64,6 +64,7 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = b0 + lane;
   constexpr int NOUT = (OP == PACK_VORDIV) ? 2 : 1;
+#pragma unroll
   for (int mi = warp; mi < kMC; mi += 8) {
     const int m = m0 + mi;
     double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
@@ -116,29 +117,60 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   }
 }
 
+// Which staged runs an unpack operator reads.  A run is (input, degree offset
+// dn = -1/0/+1, cos/sin part); runs are numbered in*6 + (dn+1)*2 + part.
+template <int OP>
+__host__ __device__ constexpr bool unpack_needs(int in, int dn)
+{
+  return OP == UNPACK_PLAIN || OP == UNPACK_GRADLAMBDA ? (in == 0 && dn == 0)
+       : OP == UNPACK_GRADMU                          ? (in == 0 && dn != 0)
+       : OP == UNPACK_ALPHA                           ? (in == 0 ? dn == 0 : dn != 0)
+                                                      : true;  // VORDIV2UV
+}
+template <int OP>
+__host__ __device__ constexpr int unpack_slot(int run)  // compact shared-memory slot of a needed run
+{
+  int s = 0;
+  for (int r = 0; r < run; ++r) s += unpack_needs<OP>(r / 6, (r % 6) / 2 - 1) ? 1 : 0;
+  return s;
+}
+template <int OP>
+__host__ __device__ constexpr int unpack_nslots() { return unpack_slot<OP>(12); }
+
 template <int OP>
 __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
 {
   constexpr int NIN = (OP == UNPACK_ALPHA || OP == UNPACK_VORDIV2UV) ? 2 : 1;
-  extern __shared__ double ws_dyn[];  // [input][(dn+1)*2 + sin][m][b]
-  auto ws = reinterpret_cast<double(*)[6][kMC][kBC + 1]>(ws_dyn);
+  extern __shared__ double ws_dyn[];  // [slot][m][b]
+  auto ws = reinterpret_cast<double(*)[kMC][kBC + 1]>(ws_dyn);
   const int2 t = a.tiles[blockIdx.x];
   const int n = t.x, m0 = t.y;
   const int b0 = blockIdx.y * kBC;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  // stage the needed SPML entries: degrees n-1..n+1, orders m0..m0+31, both parts
-  for (int q = warp; q < NIN * 6 * kBC; q += 8) {
-    const int in = q / (6 * kBC), rem = q - in * 6 * kBC;
-    const int run = rem / kBC, bi = rem - run * kBC;
-    const int nn = n + run / 2 - 1, sn = run & 1;
-    const int m = m0 + lane, bb = b0 + bi;
-    double val = 0.0;
+  // Stage the SPML entries the operator reads (degrees n-1..n+1 as needed,
+  // orders m0..m0+31, both parts).  Warp w takes field-levels b0 + 8i' + w of
+  // every run, so the run of each unrolled load is a compile-time constant;
+  // all loads of a warp are issued before any of them is stored.
+  constexpr int PER = NIN * 6 * (kBC / 8);
+  double val[PER];
+  const int m = m0 + lane;
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int run = i / (kBC / 8), in = run / 6, dn = (run % 6) / 2 - 1, sn = run & 1;
+    val[i] = 0.0;
+    if (!unpack_needs<OP>(in, dn)) continue;
+    const int nn = n + dn, bb = b0 + 8 * (i % (kBC / 8)) + warp;
     if (nn >= 0 && nn <= a.N && m <= nn && bb < a.nb && !(sn && m == 0)) {
       const double *w = (in == 0) ? a.w0 : a.w1;
       const long long l = (long long)nn * (nn + 1) + (sn ? -m : m);
-      val = __ldg(w + (long long)bb * a.L + l);
+      val[i] = __ldg(w + (long long)bb * a.L + l);
     }
-    ws[in][run][lane][bi] = val;
+  }
+#pragma unroll
+  for (int i = 0; i < PER; ++i) {
+    const int run = i / (kBC / 8);
+    if (unpack_needs<OP>(run / 6, (run % 6) / 2 - 1))
+      ws[unpack_slot<OP>(run)][lane][8 * (i % (kBC / 8)) + warp] = val[i];
   }
   __syncthreads();
   const int b = b0 + lane;
@@ -148,8 +180,8 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
     if (m > n || m > a.N) continue;
     const double s = (m == 0) ? 1.0 : kRSqrt2;
     auto coef = [&](int in, int dn) -> double2 {
-      const int run = (dn + 1) * 2;
-      return make_double2(ws[in][run][mi][lane] * s, ws[in][run + 1][mi][lane] * s);
+      const int run = in * 6 + (dn + 1) * 2;
+      return make_double2(ws[unpack_slot<OP>(run)][mi][lane] * s, ws[unpack_slot<OP>(run + 1)][mi][lane] * s);
     };
     auto R = [&](int in, double mult0) -> double2 {  // (n+2) eps_{n+1} x_{n+1} - (n-1) eps_n x_{n-1}, x scaled per degree
       const double ep = (n + 2) * eps_at(a, m, n + 1), em = (n - 1) * eps_at(a, m, n);
@@ -270,19 +302,19 @@ int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1,
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
   a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
   dim3 grid(p->n_spec_tiles, (nb + kBC - 1) / kBC);
-  const size_t one = sizeof(double) * 6 * kMC * (kBC + 1);
+  const size_t one = sizeof(double) * kMC * (kBC + 1);  // one staged run
   cudaError_t e = cudaSuccess;
-  auto run = [&](auto kern, int nin) {
-    const size_t smem = one * nin;
+  auto run = [&](auto kern, int nslots) {
+    const size_t smem = one * nslots;
     if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) kern<<<grid, 256, smem, s>>>(a);
   };
   switch (op) {
-  case UNPACK_PLAIN: run(k_unpack<UNPACK_PLAIN>, 1); break;
-  case UNPACK_GRADLAMBDA: run(k_unpack<UNPACK_GRADLAMBDA>, 1); break;
-  case UNPACK_GRADMU: run(k_unpack<UNPACK_GRADMU>, 1); break;
-  case UNPACK_ALPHA: run(k_unpack<UNPACK_ALPHA>, 2); break;
-  case UNPACK_VORDIV2UV: run(k_unpack<UNPACK_VORDIV2UV>, 2); break;
+  case UNPACK_PLAIN: run(k_unpack<UNPACK_PLAIN>, unpack_nslots<UNPACK_PLAIN>()); break;
+  case UNPACK_GRADLAMBDA: run(k_unpack<UNPACK_GRADLAMBDA>, unpack_nslots<UNPACK_GRADLAMBDA>()); break;
+  case UNPACK_GRADMU: run(k_unpack<UNPACK_GRADMU>, unpack_nslots<UNPACK_GRADMU>()); break;
+  case UNPACK_ALPHA: run(k_unpack<UNPACK_ALPHA>, unpack_nslots<UNPACK_ALPHA>()); break;
+  case UNPACK_VORDIV2UV: run(k_unpack<UNPACK_VORDIV2UV>, unpack_nslots<UNPACK_VORDIV2UV>()); break;
   default: set_error("unpack: unknown operator"); return SHT_ERR_INVALID_ARG;
   }
   if (e != cudaSuccess) return cuda_fail(e, "k_unpack smem attribute");
