@@ -85,42 +85,47 @@ __device__ __forceinline__ void dmma(double (&d)[2], double a, double b)
 }
 
 // Stage the Legendre rows of the pair: m_a rows at 0.., m_b rows right after.
+template <int JH>
 __device__ void load_pair_P(const V2Args &a, const Geo &g, double *Pbuf, int ma, int mb)
 {
+  constexpr int cpr = JH / 2;  // 16-byte chunks per row
   const int Ra = a.N + 2 - ma, Rb = (mb >= 0) ? a.N + 2 - mb : 0;
-  const int cpr = a.JH / 2;  // 16-byte chunks per row
   const int total = (Ra + Rb) * cpr;
   const double *Pa = a.P + a.poff[ma];
   const double *Pb = (mb >= 0) ? a.P + a.poff[mb] : Pa;
   for (int q = threadIdx.x; q < total; q += kT) {
-    const int row = q / cpr, ch = q - row * cpr;
-    const double *src = (row < Ra) ? Pa + (long long)row * a.JH : Pb + (long long)(row - Ra) * a.JH;
+    const int row = q / cpr, ch = q % cpr;
+    const double *src = (row < Ra) ? Pa + (long long)row * JH : Pb + (long long)(row - Ra) * JH;
     cp16(Pbuf + row * g.PS + 2 * ch, src + 2 * ch, true);
   }
 }
 
 // ------------------------------------------------------------------ analysis
+// Thread q copies latitude (q mod J) of column rows q/J, q/J + kT/J, ...
+template <int JH>
 __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
 {
-  const int nm = (mb >= 0) ? 2 : 1;
-  const int total = nm * kCT * a.J;
-  for (int q = threadIdx.x; q < total; q += kT) {
-    const int mi = q / (kCT * a.J), rem = q - mi * kCT * a.J;
-    const int b = rem / a.J, j = rem - b * a.J;
+  constexpr int J = 2 * JH, RSTEP = kT / J;  // column rows covered per pass
+  const int nrow = (mb >= 0) ? 2 * kCT : kCT;
+  const int j = threadIdx.x % J;
+#pragma unroll 4
+  for (int row = threadIdx.x / J; row < nrow; row += RSTEP) {
+    const int mi = row / kCT, b = row % kCT;
     const int m = mi ? mb : ma;
     const bool ok = col0 + b < a.ncol;
-    const double2 *src = ok ? a.F + ((long long)m * a.ncol + col0 + b) * a.J + j : a.F;
-    cp16(buf + (mi * kCT + b) * g.CS + 2 * j, src, ok);
+    const double2 *src = ok ? a.F + ((long long)m * a.ncol + col0 + b) * J + j : a.F;
+    cp16(buf + row * g.CS + 2 * j, src, ok);
   }
 }
 
 // In place: row [j] of a column -> Gs at jh, Ga at JH + jh (jh = 0..JH-1)
-__device__ void combine_panels(const V2Args &a, const Geo &g, double *buf, int nm)
+template <int JH>
+__device__ void combine_panels(const Geo &g, double *buf, int nm)
 {
-  const int JH = a.JH, half = JH / 2;
+  constexpr int half = JH / 2;
   const int total = nm * kCT * half;
   for (int q = threadIdx.x; q < total; q += kT) {
-    const int row = q / half, jh = q - row * half;
+    const int row = q / half, jh = q % half;
     double2 *G = reinterpret_cast<double2 *>(buf + row * g.CS);
     const int jq = JH - 1 - jh;
     const double2 s0 = G[jh], s1 = G[jq];            // south rows JH-1-jq, JH-1-jh
@@ -132,10 +137,11 @@ __device__ void combine_panels(const V2Args &a, const Geo &g, double *buf, int n
   }
 }
 
+template <int JH>
 __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
 {
   extern __shared__ __align__(16) double sm[];
-  const Geo g = make_geo(a.N, a.J);
+  const Geo g = make_geo(a.N, 2 * JH);
   double *Pbuf = sm;
   double *const G0 = sm + g.prow_cap * g.PS, *const G1 = G0 + 2 * kCT * g.CS;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -145,7 +151,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
 
   {
     const int2 pr = a.pairs[it0 / a.ntiles];
-    load_F_panels(a, g, G0, pr.x, pr.y, (it0 % a.ntiles) * kCT);
+    load_F_panels<JH>(a, g, G0, pr.x, pr.y, (it0 % a.ntiles) * kCT);
     cp_commit();
   }
   int cur = -1;
@@ -154,20 +160,20 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
     const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCT;
     const int2 pr = a.pairs[pidx];
     if (pidx != cur) {
-      load_pair_P(a, g, Pbuf, pr.x, pr.y);
+      load_pair_P<JH>(a, g, Pbuf, pr.x, pr.y);
       cur = pidx;
     }
     cp_commit();
     if (it + 1 < it1) {
       const int2 pn = a.pairs[(it + 1) / a.ntiles];
-      load_F_panels(a, g, bsel ? G0 : G1, pn.x, pn.y, ((it + 1) % a.ntiles) * kCT);
+      load_F_panels<JH>(a, g, bsel ? G0 : G1, pn.x, pn.y, ((it + 1) % a.ntiles) * kCT);
     }
     cp_commit();
     cp_wait1();
     __syncthreads();
     const int nm = (pr.y >= 0) ? 2 : 1;
     double *const Gcur = bsel ? G1 : G0;
-    combine_panels(a, g, Gcur, nm);
+    combine_panels<JH>(g, Gcur, nm);
     __syncthreads();
 
     // jobs: (band, parity, 16-row group)
@@ -183,7 +189,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
       else { mi = 1; par = 1; gi = job - gEa - gOa - gEb; }
       const int m = mi ? pr.y : pr.x, R = mi ? Rb : Ra;
       const double *Pm = Pbuf + (mi ? Ra : 0) * g.PS;
-      const double *G = Gcur + mi * kCT * g.CS + (par ? 2 * a.JH : 0);
+      const double *G = Gcur + mi * kCT * g.CS + (par ? 2 * JH : 0);
       const int r0 = par + 2 * (16 * gi + (lane >> 2));
       const int r1 = r0 + 16;
       const double *pa0 = Pm + min(r0, R - 1) * g.PS + (lane & 3);
@@ -194,8 +200,8 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
       for (int t = 0; t < 2; ++t)
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) acc[t][nt][0] = acc[t][nt][1] = 0.0;
-#pragma unroll 4
-      for (int kb = 0; kb < a.JH; kb += 4) {
+#pragma unroll
+      for (int kb = 0; kb < JH; kb += 4) {
         const double a0 = pa0[kb], a1 = pa1[kb];
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
@@ -222,25 +228,31 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
 }
 
 // ----------------------------------------------------------------- synthesis
+// Thread q copies column (q mod kCT) of coefficient rows q/kCT, q/kCT + kT/kCT, ...
 __device__ void load_S_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
 {
+  constexpr int RSTEP = kT / kCT;
   const int nm = (mb >= 0) ? 2 : 1;
-  const int total = nm * g.arow_cap * kCT;
-  for (int q = threadIdx.x; q < total; q += kT) {
-    const int mi = q / (g.arow_cap * kCT), rem = q - mi * g.arow_cap * kCT;
-    const int r = rem / kCT, c = rem - r * kCT;
-    const int m = mi ? mb : ma;
-    const int R = a.N + 2 - m;
-    const bool ok = (r < R) && (col0 + c < a.ncol);
-    const double2 *src = ok ? a.Sc + ((long long)a.rowoff[m] + r) * a.ncol + col0 + c : a.Sc;
-    cp16(buf + (mi * g.arow_cap + r) * g.AS + 2 * c, src, ok);
+  const int c = threadIdx.x % kCT;
+  const bool cok = col0 + c < a.ncol;
+  const int Ra = a.N + 2 - ma, Rb = (mb >= 0) ? a.N + 2 - mb : 0;
+  const double2 *Sa = a.Sc + (long long)a.rowoff[ma] * a.ncol + col0 + c;
+  const double2 *Sb = (mb >= 0) ? a.Sc + (long long)a.rowoff[mb] * a.ncol + col0 + c : Sa;
+#pragma unroll 4
+  for (int row = threadIdx.x / kCT; row < nm * g.arow_cap; row += RSTEP) {
+    const bool second = row >= g.arow_cap;
+    const int r = second ? row - g.arow_cap : row;
+    const bool ok = cok && r < (second ? Rb : Ra);
+    const double2 *src = ok ? (second ? Sb : Sa) + (long long)r * a.ncol : a.Sc;
+    cp16(buf + row * g.AS + 2 * c, src, ok);
   }
 }
 
+template <int JH>
 __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
 {
   extern __shared__ __align__(16) double sm[];
-  const Geo g = make_geo(a.N, a.J);
+  const Geo g = make_geo(a.N, 2 * JH);
   double *Pbuf = sm;
   const int abuf = 2 * g.arow_cap * g.AS;
   double *const A0 = sm + g.prow_cap * g.PS, *const A1 = A0 + abuf;
@@ -249,9 +261,9 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
   const int it1 = min(a.nitems, it0 + a.per_cta);
   if (it0 >= it1) return;
   // units: (latitude tile of 8, group of column tiles) over the 8 warps
-  const int ntj = a.JH / 8;               // 2, 4 or 8
-  const int ngrp = kW / ntj;              // 4, 2 or 1
-  const int nnt = 4 / ngrp;               // column tiles (of 8 reals) per unit
+  constexpr int ntj = JH / 8;             // 2, 4 or 8
+  constexpr int ngrp = kW / ntj;          // 4, 2 or 1
+  constexpr int nnt = 4 / ngrp;           // column tiles (of 8 reals) per unit
   const int jt = warp % ntj, grp = warp / ntj;
 
   {
@@ -265,7 +277,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
     const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCT;
     const int2 pr = a.pairs[pidx];
     if (pidx != cur) {
-      load_pair_P(a, g, Pbuf, pr.x, pr.y);
+      load_pair_P<JH>(a, g, Pbuf, pr.x, pr.y);
       cur = pidx;
     }
     cp_commit();
@@ -307,10 +319,10 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
         if (q >= nnt) continue;
         const int c = col0 + 4 * (grp * nnt + q) + (lane & 3);
         if (c >= a.ncol) continue;
-        double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * a.J;
+        double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
         const double er = acc[0][q][0], ei = acc[0][q][1], orr = acc[1][q][0], oi = acc[1][q][1];
-        Fc[a.JH + jh] = make_double2(er + orr, ei + oi);
-        Fc[a.JH - 1 - jh] = make_double2(er - orr, ei - oi);
+        Fc[JH + jh] = make_double2(er + orr, ei + oi);
+        Fc[JH - 1 - jh] = make_double2(er - orr, ei - oi);
       }
     }
     __syncthreads();
@@ -349,7 +361,13 @@ int launch_pair(const sht_plan *p, bool inverse, const double2 *in, int ncol, do
   a.ntiles = (ncol + kCT - 1) / kCT;
   a.nitems = npairs * a.ntiles;
   const size_t smem = inverse ? inv_smem(p->N, p->J) : fwd_smem(p->N, p->J);
-  auto kern = inverse ? k_leg_inv_pair : k_leg_fwd_pair;
+  void (*kern)(V2Args) = nullptr;
+  switch (p->JH) {
+  case 16: kern = inverse ? k_leg_inv_pair<16> : k_leg_fwd_pair<16>; break;
+  case 32: kern = inverse ? k_leg_inv_pair<32> : k_leg_fwd_pair<32>; break;
+  case 64: kern = inverse ? k_leg_inv_pair<64> : k_leg_fwd_pair<64>; break;
+  default: set_error("legendre: latitude count outside the paired kernels"); return SHT_ERR_UNSUPPORTED_SIZE;
+  }
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "legendre pair smem attribute");
   int per_sm = 0;
