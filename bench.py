@@ -182,6 +182,64 @@ def cpu_baseline(nb, seconds=10.0):
 
 
 # ------------------------------------------------------------------ ours
+def bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world):
+    """Config C3: 64 independent instances, truncations T21/T42/T85/T170 in
+    ratio 8:4:2:1, levels U[10, 60] x 3-8 fields each, seeded spectra
+    ~(n+1)^-1.5.  One step = one round trip of every instance = one replay of
+    the batch's CUDA graph (sht_multi_run), timed with CUDA events on the
+    launching stream, L2 flushed between steps outside the events."""
+    grids = ("T21", "T42", "T85", "T170")
+    plans = {g: P.SpmlUtil(*W.GRIDS[g][:2], 1, W.GRIDS[g][2], None, RADIUS) for g in grids}
+    arrays = []
+    for k, d in enumerate(W.mixed_instances(64)):
+        p = plans[d["grid"]]
+        nb = d["levels"] * d["fields"]
+        w0 = W.seeded_spectra_torch(p.nm, nb, 1.5, dev, seed=W.SEED + k)
+        arrays.append((p, torch.empty_like(w0), torch.empty((nb, p.jm, p.im), dtype=torch.float64, device=dev), w0))
+    total = sum(a[3].shape[0] for a in arrays)
+    stream = torch.cuda.current_stream(dev)
+    out = {"workload": "C3: 64 instances T21/T42/T85/T170 (8:4:2:1), levels U[10,60] x fields 3-8",
+           "field_levels_per_step": total,
+           "instances_per_grid": {g: sum(1 for a in arrays if a[0] is plans[g]) for g in grids}}
+    for mode, allow_split in (("fp64", False), ("split_allowed", True)):
+        m = P.MultiTransform()
+        for p, wa, xya, _ in arrays:
+            m.add(p, wa, xya)
+        t0 = time.perf_counter()
+        m.build(autotune=True, allow_split=allow_split)
+        build_s = time.perf_counter() - t0
+        for _, wa, _, w0 in arrays:
+            wa.copy_(w0)
+        m.set_stream(stream)
+        for _ in range(args.warmup):
+            flush.zero_()
+            m.run(P.SHT_MULTI_ROUND_TRIP)
+        torch.cuda.synchronize()
+        evs = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            m.run(P.SHT_MULTI_ROUND_TRIP)
+            e1.record(stream)
+            evs.append((e0, e1))
+        m.synchronize()
+        tot = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs))
+        err = max(_rel(wa.cpu().numpy(), w0.cpu().numpy()) for _, wa, _, w0 in arrays)
+        names = {0: "fp64", 1: "split"}
+        out[mode] = {"value": world * total * args.steps / (tot * 1e-3), "unit": UNIT,
+                     "ms_per_step": tot / args.steps, "kernels_per_step": m.kernels(P.SHT_MULTI_ROUND_TRIP),
+                     "graph_launches_per_step": 1, "build_s": build_s, "relerr": err,
+                     "groups": [{"grid": g, "field_levels": x["ncol"], "precision": names[x["precision"]],
+                                 "legendre_kernel": {0: "auto", 1: "per-band chunked", 2: "paired persistent"}
+                                 [x["legendre_kernel"]], "tuned_round_trip_ms": x["tuned_ms"]}
+                                for g, x in zip(sorted(grids, key=lambda g: plans[g]._h.value), m.groups())]}
+        m.close()
+    for p in plans.values():
+        p.final()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -192,6 +250,7 @@ def main():
     ap.add_argument("--nb", type=int, default=0, help="field-levels (default 480)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-multi", action="store_true", help="skip the C3 multi-instance measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -357,6 +416,8 @@ def main():
                "path": "sht_xya_wa + sht_wa_xya on pinned host arrays (synchronous C-ABI calls, host clock)",
                "relerr": _rel(wo.numpy(), wh.numpy())}
 
+    multi = None if args.no_multi else bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(nb)
@@ -381,6 +442,7 @@ def main():
             "e2e": e2e,
             "clocks": head["clocks"],
             "gpu_launches": head["launches"],
+            "multi_instance": multi,
         }
         print(json.dumps(rec))
     sht.final()

@@ -311,6 +311,27 @@ void free_plan(sht_plan *p)
 }
 
 }  // namespace
+
+// Plain analysis / synthesis over per-column pointer tables with caller-owned
+// Fourier (F) and internal spectral (S) buffers: the multi-instance batches.
+int run_analysis_cols(sht_plan *p, const double *const *gcol, int ncol, double *const *wcol, double2 *F,
+                      double2 *S, cudaStream_t s)
+{
+  int rc;
+  if ((rc = launch_fft_fwd(p, nullptr, nullptr, ncol, ncol, F, ncol, 0, RS_FWD_PLAIN, s, gcol))) return rc;
+  if ((rc = leg_fwd(p, F, ncol, S, s))) return rc;
+  return launch_pack(p, PACK_PLAIN, S, ncol, ncol, nullptr, nullptr, s, wcol);
+}
+
+int run_synthesis_cols(sht_plan *p, const double *const *wcol, int ncol, double *const *gcol, double2 *F,
+                       double2 *S, cudaStream_t s)
+{
+  int rc;
+  if ((rc = launch_unpack(p, UNPACK_PLAIN, nullptr, nullptr, ncol, S, ncol, s, wcol))) return rc;
+  if ((rc = leg_inv(p, S, ncol, F, s))) return rc;
+  return launch_fft_inv(p, F, ncol, 0, ncol, nullptr, nullptr, ncol, RS_INV_PLAIN, s, gcol);
+}
+
 }  // namespace sht
 
 using namespace sht;

@@ -117,6 +117,8 @@ struct FftArgs {
   const double *rowscale;
   const double2 *tw, *twI;
   int I, J, N;
+  const double *const *gcol;  // optional per-column grid sources (forward)
+  double *const *ocol;        // optional per-column grid destinations (inverse)
 };
 
 // Shared-memory plan of one thread block: the twiddle tables (2 NC entries),
@@ -183,8 +185,9 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
 
   auto issue = [&](long long t, double2 *buf) {
     const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT;
-    const double2 *src = reinterpret_cast<const double2 *>(
-        ((col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ) + (long long)j0 * a.I);
+    const double *gb = a.gcol ? a.gcol[col]
+                     : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
+    const double2 *src = reinterpret_cast<const double2 *>(gb + (long long)j0 * a.I);
     const int nrows = min(JT, a.J - j0);
 #pragma unroll 4
     for (int q = tid; q < JT * NC; q += NT) {
@@ -357,7 +360,8 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
     }
     if (valid) {
       const long long IJ = (long long)a.I * a.J;
-      double *dst = (col < a.nsplit) ? a.o0 + (long long)col * IJ : a.o1 + (long long)(col - a.nsplit) * IJ;
+      double *dst = a.ocol ? a.ocol[col]
+                  : (col < a.nsplit) ? a.o0 + (long long)col * IJ : a.o1 + (long long)(col - a.nsplit) * IJ;
       double2 *rowp = reinterpret_cast<double2 *>(dst + (long long)j * a.I);
       const double sc = __ldg(a.rowscale + j);
 #pragma unroll
@@ -440,9 +444,10 @@ int dispatch(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t 
 }  // namespace
 
 int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
-                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s)
+                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s, const double *const *gcol)
 {
   FftArgs a{};
+  a.gcol = gcol;
   a.g0 = g0; a.g1 = g1 ? g1 : g0; a.nsplit = nsplit; a.ncol = ncol;
   a.F = F; a.ncolF = ncolF; a.colF0 = colF0;
   a.rowscale = p->d_rowscale + (size_t)rs * p->J;
@@ -452,9 +457,10 @@ int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int ns
 }
 
 int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, int ncol,
-                   double *g0, double *g1, int nsplit, int rs, cudaStream_t s)
+                   double *g0, double *g1, int nsplit, int rs, cudaStream_t s, double *const *ocol)
 {
   FftArgs a{};
+  a.ocol = ocol;
   a.o0 = g0; a.o1 = g1 ? g1 : g0; a.nsplit = nsplit; a.ncol = ncol;
   a.Fc = F; a.ncolF = ncolF; a.colF0 = colF0;
   a.rowscale = p->d_rowscale + (size_t)rs * p->J;

@@ -118,13 +118,17 @@ void count_launch(int n = 1);
 int build_tables(sht_plan *p);
 
 // --- longitude transforms (sht_fft.cu)
-// grid (up to two source arrays: columns [0, nsplit) from g0, the rest from g1)
-// -> F[m][colF0 + col][j], scaled per row by rowscale table `rs`.
+// grid (up to two source arrays: columns [0, nsplit) from g0, the rest from g1;
+// or, when gcol is given, column c at gcol[c]) -> F[m][colF0 + col][j],
+// scaled per row by rowscale table `rs`.
 int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
-                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s);
-// F -> grid (two destinations split at nsplit), scaled per row by `rs`.
+                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s,
+                   const double *const *gcol = nullptr);
+// F -> grid (two destinations split at nsplit, or column c at ocol[c]),
+// scaled per row by `rs`.
 int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, int ncol,
-                   double *g0, double *g1, int nsplit, int rs, cudaStream_t s);
+                   double *g0, double *g1, int nsplit, int rs, cudaStream_t s,
+                   double *const *ocol = nullptr);
 
 // --- Legendre contraction, FP64 (sht_legendre.cu)
 int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
@@ -142,13 +146,23 @@ void free_split_tables(sht_plan *p);
 bool split_supported(const sht_plan *p);
 int split_error_status(sht_plan *p);  // reads and clears the device error word (synchronous)
 
+// --- column-table pipelines (sht_capi.cu), used by the multi-instance batches
+// F holds (N+1) J ncol complex values, S holds R ncol; the plan mutex is held
+// by the caller.
+int run_analysis_cols(sht_plan *p, const double *const *gcol, int ncol, double *const *wcol, double2 *F,
+                      double2 *S, cudaStream_t s);
+int run_synthesis_cols(sht_plan *p, const double *const *wcol, int ncol, double *const *gcol, double2 *F,
+                       double2 *S, cudaStream_t s);
+
 // --- spectral-side kernels (sht_spectral.cu)
 // internal S (ncolS columns; set A at col 0, set B at col nb) -> SPML wa outputs
+// (field-level b at w0 + b L, or at wcol[b] when a column table is given;
+// tables serve the single-output operators)
 int launch_pack(const sht_plan *p, int op, const double2 *S, int ncolS, int nb, double *w0,
-                double *w1, cudaStream_t s);
-// SPML inputs -> internal S (ncolS columns)
+                double *w1, cudaStream_t s, double *const *wcol = nullptr);
+// SPML inputs -> internal S (ncolS columns); wcol as for launch_pack
 int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1, int nb,
-                  double2 *S, int ncolS, cudaStream_t s);
+                  double2 *S, int ncolS, cudaStream_t s, const double *const *wcol = nullptr);
 int launch_lapla(const sht_plan *p, const double *w, int nb, double *out, bool inverse,
                  cudaStream_t s);
 int launch_diffuse(const sht_plan *p, double *w, int nb, const double *coef, double dt,

@@ -43,6 +43,8 @@ struct SpecArgs {
   const int *rowoff;
   const double *eps;      // [m][n], n = 0..N+2
   const int2 *tiles;      // (n, m0) per tile
+  double *const *ocol;        // optional per-field-level pack destinations
+  const double *const *icol;  // optional per-field-level unpack sources
 };
 
 __device__ __forceinline__ double eps_at(const SpecArgs &a, int m, int n)
@@ -110,9 +112,9 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
     if (bb >= a.nb || m > n) continue;
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
-      double *w = (o == 0) ? a.o0 : a.o1;
-      w[(long long)bb * a.L + lc + m] = out[o][0][mi][bi];
-      if (m > 0) w[(long long)bb * a.L + lc - m] = out[o][1][mi][bi];
+      double *w = (o == 0 && a.ocol) ? a.ocol[bb] : ((o == 0) ? a.o0 : a.o1) + (long long)bb * a.L;
+      w[lc + m] = out[o][0][mi][bi];
+      if (m > 0) w[lc - m] = out[o][1][mi][bi];
     }
   }
 }
@@ -161,9 +163,9 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
     if (!unpack_needs<OP>(in, dn)) continue;
     const int nn = n + dn, bb = b0 + 8 * (i % (kBC / 8)) + warp;
     if (nn >= 0 && nn <= a.N && m <= nn && bb < a.nb && !(sn && m == 0)) {
-      const double *w = (in == 0) ? a.w0 : a.w1;
+      const double *w = (in == 0 && a.icol) ? a.icol[bb] : ((in == 0) ? a.w0 : a.w1) + (long long)bb * a.L;
       const long long l = (long long)nn * (nn + 1) + (sn ? -m : m);
-      val[i] = __ldg(w + (long long)bb * a.L + l);
+      val[i] = __ldg(w + l);
     }
   }
 #pragma unroll
@@ -272,10 +274,11 @@ __global__ void __launch_bounds__(256) k_lonlat(const double *__restrict__ g, in
 }  // namespace
 
 int launch_pack(const sht_plan *p, int op, const double2 *S, int ncolS, int nb, double *w0,
-                double *w1, cudaStream_t s)
+                double *w1, cudaStream_t s, double *const *wcol)
 {
   if (nb <= 0) return SHT_OK;
   SpecArgs a{};
+  a.ocol = wcol;
   a.S = S; a.ncolS = ncolS; a.o0 = w0; a.o1 = w1 ? w1 : w0;
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
   a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
@@ -294,10 +297,11 @@ int launch_pack(const sht_plan *p, int op, const double2 *S, int ncolS, int nb, 
 }
 
 int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1, int nb,
-                  double2 *S, int ncolS, cudaStream_t s)
+                  double2 *S, int ncolS, cudaStream_t s, const double *const *wcol)
 {
   if (nb <= 0) return SHT_OK;
   SpecArgs a{};
+  a.icol = wcol;
   a.So = S; a.ncolS = ncolS; a.w0 = w0; a.w1 = w1 ? w1 : w0;
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
   a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;

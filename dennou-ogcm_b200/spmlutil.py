@@ -30,6 +30,8 @@ SHT_OK = 0
 SHT_PREC_FP64 = 0
 SHT_PREC_SPLIT = 1
 SHT_OPT_LEGENDRE_KERNEL = 1
+SHT_MULTI_SYNTHESIS, SHT_MULTI_ANALYSIS, SHT_MULTI_ROUND_TRIP = 1, 2, 3
+SHT_MULTI_AUTOTUNE, SHT_MULTI_ALLOW_SPLIT, SHT_MULTI_NO_GRAPH = 1, 2, 4
 
 _D = ctypes.POINTER(ctypes.c_double)
 _VP = ctypes.c_void_p
@@ -94,6 +96,17 @@ def load_library(path: str | None = None):
     for suf in ("", "_dev"):
         getattr(lib, "sht_wa_diffuse" + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
     lib.sht_roundtrip_diffuse_dev.argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
+    lib.sht_multi_create.argtypes = [ctypes.POINTER(_VP)]
+    lib.sht_multi_add.argtypes = [_VP, _VP, ctypes.c_int, _VP, _VP, ctypes.POINTER(ctypes.c_int)]
+    lib.sht_multi_build.argtypes = [_VP, ctypes.c_int]
+    lib.sht_multi_run.argtypes = [_VP, ctypes.c_int]
+    lib.sht_multi_synchronize.argtypes = [_VP]
+    lib.sht_multi_set_stream.argtypes = [_VP, _VP]
+    lib.sht_multi_groups.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
+    lib.sht_multi_group_info.argtypes = [_VP, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 3 + \
+        [ctypes.POINTER(ctypes.c_float)]
+    lib.sht_multi_kernels.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.sht_multi_destroy.argtypes = [_VP]
     _lib = lib
     return lib
 
@@ -372,3 +385,82 @@ class SpmlUtil:
                                              _VP(filt.data_ptr()) if filt is not None else None),
                "roundtrip_diffuse_")
         return xya
+
+
+class MultiTransform:
+    """Many independent transform instances run as one step (sht_multi_* C-ABI).
+
+    Each instance is (plan, wa, xya): a SpmlUtil plan and CUDA torch tensors
+    wa (nb, lm) and xya (nb, jm, im), FP64, contiguous.  build() groups the
+    instances per plan, optionally tunes the Legendre variant of every plan and
+    captures each step kind as a CUDA graph; run() replays one step on the
+    batch's own stream.  build() runs steps on the registered arrays, so fill
+    them afterwards.  The reference keeps a single grid per process; this is
+    the batched step API of the transform path.
+    """
+
+    def __init__(self):
+        self._lib = load_library()
+        h = _VP()
+        _check(self._lib.sht_multi_create(ctypes.byref(h)), "sht_multi_create")
+        self._h = h
+        self._keep = []  # the registered tensors must stay alive and in place
+
+    def add(self, plan: "SpmlUtil", wa, xya) -> int:
+        if not (_is_torch_cuda(wa) and _is_torch_cuda(xya)):
+            raise TypeError("MultiTransform instances take CUDA torch tensors")
+        import torch
+        if wa.dtype != torch.float64 or xya.dtype != torch.float64 or not (wa.is_contiguous() and xya.is_contiguous()):
+            raise TypeError("wa and xya must be contiguous float64 tensors")
+        nb = wa.shape[0]
+        if tuple(wa.shape) != (nb, plan.lm) or tuple(xya.shape) != (nb, plan.jm, plan.im):
+            raise ValueError("wa must be (nb, lm) and xya (nb, jm, im) for the plan")
+        idx = ctypes.c_int()
+        _check(self._lib.sht_multi_add(self._h, plan._h, int(nb), wa.data_ptr(), xya.data_ptr(), ctypes.byref(idx)),
+               "sht_multi_add")
+        self._keep.append((plan, wa, xya))
+        return idx.value
+
+    def build(self, autotune: bool = True, allow_split: bool = False, graph: bool = True):
+        flags = (SHT_MULTI_AUTOTUNE if autotune else 0) | (SHT_MULTI_ALLOW_SPLIT if allow_split else 0) | \
+            (0 if graph else SHT_MULTI_NO_GRAPH)
+        _check(self._lib.sht_multi_build(self._h, flags), "sht_multi_build")
+
+    def run(self, what: int = SHT_MULTI_ROUND_TRIP):
+        _check(self._lib.sht_multi_run(self._h, int(what)), "sht_multi_run")
+
+    def synchronize(self):
+        _check(self._lib.sht_multi_synchronize(self._h), "sht_multi_synchronize")
+
+    def set_stream(self, stream):
+        """Order runs on a torch CUDA stream (its handle; the default stream is 0)."""
+        _check(self._lib.sht_multi_set_stream(self._h, stream.cuda_stream), "sht_multi_set_stream")
+
+    def groups(self):
+        """Per plan group: dict(ncol, precision, legendre_kernel, tuned_ms)."""
+        n = ctypes.c_int()
+        _check(self._lib.sht_multi_groups(self._h, ctypes.byref(n)), "sht_multi_groups")
+        out = []
+        for g in range(n.value):
+            nc, pr, lk, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
+            _check(self._lib.sht_multi_group_info(self._h, g, ctypes.byref(nc), ctypes.byref(pr), ctypes.byref(lk),
+                                                  ctypes.byref(ms)), "sht_multi_group_info")
+            out.append(dict(ncol=nc.value, precision=pr.value, legendre_kernel=lk.value, tuned_ms=ms.value))
+        return out
+
+    def kernels(self, what: int = SHT_MULTI_ROUND_TRIP) -> int:
+        n = ctypes.c_int()
+        _check(self._lib.sht_multi_kernels(self._h, int(what), ctypes.byref(n)), "sht_multi_kernels")
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _check(self._lib.sht_multi_destroy(self._h), "sht_multi_destroy")
+            self._h = None
+            self._keep = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -236,6 +236,61 @@ SHT_API int sht_roundtrip_diffuse_dev(sht_plan *plan, double *xya, int nb, const
 SHT_API int sht_wa_xya_dev_noalloc(sht_plan *plan, const double *xya, int nb, double *wa);
 SHT_API unsigned long long sht_noalloc_scratch_bytes(void);
 
+/* ------------------------------------------------ multi-instance batches
+ * Many independent transform instances in one step.  Each instance has its
+ * own plan (grid and truncation), field-level count nb and device arrays
+ * wa (lm x nb, SPML layout) and xya (im x jm x nb).  The instances of one
+ * plan run as a single column range through the same kernels as a batched
+ * call (per-column pointer tables, no gather copies); different plans run side
+ * by side on their own streams.  sht_multi_build groups the instances,
+ * optionally times the Legendre variants of every plan and keeps the fastest,
+ * and captures each step kind once as a CUDA graph that sht_multi_run replays.
+ *
+ * The reference holds one grid per process (SpmlUtil_mod.f90:146-160), so
+ * this has no counterpart there; it is the batched step API of the transform
+ * path (ensemble members or several resolutions in one job).
+ *
+ * Rules: the batch owns its Fourier and spectral workspaces; the plans'
+ * tables must outlive it (sht_multi_destroy before sht_final); grid arrays
+ * must be 16-byte aligned, and no array may move after sht_multi_build; runs
+ * of one batch are ordered on its own stream.  sht_multi_build runs steps on
+ * the registered arrays (warm-up and tuning, as a measuring FFT planner does),
+ * so fill them after building. */
+typedef struct sht_multi_s sht_multi;
+
+#define SHT_MULTI_SYNTHESIS 1  /* xya = xy_w(wa) for every instance */
+#define SHT_MULTI_ANALYSIS 2   /* wa = w_xy(xya) for every instance */
+#define SHT_MULTI_ROUND_TRIP 3 /* synthesis, then analysis */
+
+#define SHT_MULTI_AUTOTUNE 1    /* build: time the Legendre variants per plan, keep the fastest */
+#define SHT_MULTI_ALLOW_SPLIT 2 /* build: the tuner may choose split precision (<= 1e-11 relative) */
+#define SHT_MULTI_NO_GRAPH 4    /* build: launch stage by stage instead of replaying a graph */
+
+/* Creates an empty batch on the current device. */
+SHT_API int sht_multi_create(sht_multi **multi);
+/* Registers one instance; returns its index through instance (may be NULL). */
+SHT_API int sht_multi_add(sht_multi *multi, sht_plan *plan, int nb, double *wa, double *xya, int *instance);
+/* Groups, sizes workspaces, tunes (flags above) and captures the graphs. */
+SHT_API int sht_multi_build(sht_multi *multi, int flags);
+/* Enqueues one step (SHT_MULTI_SYNTHESIS / _ANALYSIS / _ROUND_TRIP) on the
+ * batch's stream and returns. */
+SHT_API int sht_multi_run(sht_multi *multi, int what);
+/* Stream the runs are enqueued on (a cudaStream_t as void*; NULL = the
+ * legacy default stream).  Until set, runs go to a stream the batch owns.  A
+ * replay is ordered after earlier work on that stream. */
+SHT_API int sht_multi_set_stream(sht_multi *multi, void *stream);
+/* Waits for the batch's stream and reports device-side errors. */
+SHT_API int sht_multi_synchronize(sht_multi *multi);
+/* Number of plan groups, and per group: columns (total field-levels), the
+ * precision and Legendre kernel option in use, and the tuned round-trip time
+ * in ms (0 when not tuned).  NULL outputs are skipped. */
+SHT_API int sht_multi_groups(const sht_multi *multi, int *ngroups);
+SHT_API int sht_multi_group_info(const sht_multi *multi, int group, int *ncol, int *precision,
+                                 int *legendre_kernel, float *tuned_ms);
+/* Kernel launches one sht_multi_run(what) replays. */
+SHT_API int sht_multi_kernels(const sht_multi *multi, int what, int *nkernels);
+SHT_API int sht_multi_destroy(sht_multi *multi);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /* Device time in milliseconds of the kernels of the last *_dev call, summed

@@ -68,3 +68,22 @@ def test_init_without_device_reports_no_device(cuda_available):
     h = ctypes.c_void_p()
     st = lib.sht_init(64, 32, 1, 21, ctypes.c_double(1.0), ctypes.byref(h))
     assert st == 5
+
+
+def test_multi_without_device_reports_no_device(cuda_available):
+    if cuda_available:
+        pytest.skip("a CUDA device is present")
+    lib = pkg().load_library()
+    h = ctypes.c_void_p()
+    assert lib.sht_multi_create(ctypes.byref(h)) == 5
+    assert not h.value
+
+
+def test_multi_calls_on_null_batch_fail_cleanly():
+    lib = pkg().load_library()
+    n = ctypes.c_int()
+    assert lib.sht_multi_create(None) == 1
+    assert lib.sht_multi_build(None, 0) == 1
+    assert lib.sht_multi_run(None, 3) == 1
+    assert lib.sht_multi_groups(None, ctypes.byref(n)) == 1
+    assert lib.sht_multi_destroy(None) == 1
