@@ -231,7 +231,8 @@ def bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world):
                      "ms_per_step": tot / args.steps, "kernels_per_step": m.kernels(P.SHT_MULTI_ROUND_TRIP),
                      "graph_launches_per_step": 1, "build_s": build_s, "relerr": err,
                      "groups": [{"grid": g, "field_levels": x["ncol"], "precision": names[x["precision"]],
-                                 "legendre_kernel": {0: "auto", 1: "per-band chunked", 2: "paired persistent"}
+                                 "legendre_kernel": {0: "auto", 1: "per-band", 2: "paired persistent",
+                                                     3: "latitude-chunked persistent"}
                                  [x["legendre_kernel"]], "tuned_round_trip_ms": x["tuned_ms"]}
                                 for g, x in zip(sorted(grids, key=lambda g: plans[g]._h.value), m.groups())]}
         m.close()

@@ -32,6 +32,21 @@ int cuda_fail(cudaError_t e, const char *what)
 }
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
+int device_error_status(sht_plan *p)
+{
+  int h = 0;
+  if (p->d_err) {
+    cudaError_t e = cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cuda_fail(e, "device error word");
+    if (h) {
+      cudaMemset(p->d_err, 0, sizeof(int));
+      set_error("a bounded device-side wait of the FP64 Legendre kernels timed out");
+      return h;
+    }
+  }
+  return split_error_status(p);
+}
+
 namespace {
 
 struct DeviceGuard {
@@ -293,7 +308,7 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
   if (sh.nout == 2 && (e = cudaMemcpyAsync(o1, do1, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
     return cuda_fail(e, "D2H");
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
-  if (p->precision == SHT_PREC_SPLIT && (rc = split_error_status(p))) return rc;
+  if ((rc = device_error_status(p))) return rc;
   finish_timing(p, !sh.out_grid);
   return SHT_OK;
 }
@@ -303,7 +318,7 @@ void free_plan(sht_plan *p)
   cudaFree(p->d_mu); cudaFree(p->d_wgt); cudaFree(p->d_rowscale); cudaFree(p->d_P);
   cudaFree(p->d_poff); cudaFree(p->d_rowoff); cudaFree(p->d_eps); cudaFree(p->d_tw);
   cudaFree(p->d_twI); cudaFree(p->d_rn); cudaFree(p->d_spec_tiles); cudaFree(p->d_pairs);
-  cudaFree(p->d_ws); cudaFree(p->d_io);
+  cudaFree(p->d_ws); cudaFree(p->d_io); cudaFree(p->d_err);
   free_split_tables(p);
   for (auto &ev : p->timing.ev)
     if (ev) cudaEventDestroy(ev);
@@ -398,6 +413,8 @@ int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
   cudaGetDevice(&p->device);
   int rc = SHT_OK;
   if ((e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking)) != cudaSuccess) rc = cuda_fail(e, "stream create");
+  if (!rc && ((e = cudaMalloc(&p->d_err, sizeof(int))) != cudaSuccess || (e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess))
+    rc = cuda_fail(e, "error word");
   p->stream = p->own_stream;
   for (int k = 0; k < 8 && !rc; ++k)
     if ((e = cudaEventCreate(&p->timing.ev[k])) != cudaSuccess) rc = cuda_fail(e, "event create");
@@ -491,7 +508,7 @@ int sht_set_option(sht_plan *p, int option, int value)
   std::lock_guard<std::mutex> lk(p->mtx);
   switch (option) {
   case SHT_OPT_LEGENDRE_KERNEL:
-    if (value < 0 || value > 2) { set_error("legendre kernel option must be 0, 1 or 2"); return SHT_ERR_INVALID_ARG; }
+    if (value < 0 || value > 3) { set_error("legendre kernel option must be 0, 1, 2 or 3"); return SHT_ERR_INVALID_ARG; }
     p->leg_kernel = value;
     return SHT_OK;
   default: set_error("unknown option"); return SHT_ERR_INVALID_ARG;
@@ -525,7 +542,7 @@ int sht_synchronize(sht_plan *p)
   DeviceGuard g(p->device);
   cudaError_t e = cudaStreamSynchronize(p->stream);
   if (e != cudaSuccess) return cuda_fail(e, "synchronize");
-  return split_error_status(p);
+  return device_error_status(p);
 }
 
 int sht_set_timing(sht_plan *p, int on)

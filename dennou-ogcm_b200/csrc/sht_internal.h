@@ -70,7 +70,7 @@ struct sht_plan_s {
   cudaStream_t stream = nullptr;      // stream used by all work of the plan
   cudaStream_t own_stream = nullptr;  // stream created by sht_init (destroyed by sht_final)
   int precision = SHT_PREC_FP64;
-  int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 chunked per-band, 2 paired persistent
+  int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent
 
   // device tables
   double *d_mu = nullptr, *d_wgt = nullptr, *d_rowscale = nullptr;
@@ -101,6 +101,8 @@ struct sht_plan_s {
 
   // split-precision tables (built lazily)
   void *tc_tables = nullptr;
+  // device error word of the bounded waits in the FP64 kernels (0 = none)
+  int *d_err = nullptr;
 
   std::mutex mtx;
   sht::Timing timing;
@@ -131,6 +133,7 @@ int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, in
                    double *const *ocol = nullptr);
 
 // --- Legendre contraction, FP64 (sht_legendre.cu)
+int pick_fp64_kernel(const sht_plan *p);  // 1 per-band, 2 paired, 3 latitude-chunked
 int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 
@@ -139,12 +142,19 @@ bool leg_pair_supported(const sht_plan *p);
 int launch_leg_fwd_pair(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_pair(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 
+// --- persistent latitude-chunked FP64 contraction for large grids (sht_legendre_v3.cu)
+bool leg_chunk_supported(const sht_plan *p);
+int launch_leg_fwd_chunk(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
+int launch_leg_inv_chunk(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
+
 // --- Legendre contraction, split precision on tcgen05 (sht_legendre_tc.cu)
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_split(sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 void free_split_tables(sht_plan *p);
 bool split_supported(const sht_plan *p);
 int split_error_status(sht_plan *p);  // reads and clears the device error word (synchronous)
+// Reads and clears every device error word of the plan (synchronous).
+int device_error_status(sht_plan *p);
 
 // --- column-table pipelines (sht_capi.cu), used by the multi-instance batches
 // F holds (N+1) J ncol complex values, S holds R ncol; the plan mutex is held

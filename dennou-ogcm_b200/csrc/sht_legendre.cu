@@ -327,10 +327,30 @@ int launch(K kern, dim3 grid, size_t smem, cudaStream_t s, const LegArgs &args, 
 }
 }  // namespace
 
+// Kernel for the plan's SHT_OPT_LEGENDRE_KERNEL setting: 1 per-band (this
+// file), 2 paired persistent, 3 latitude-chunked persistent; 0 picks the
+// paired kernel where the pair fits in shared memory, else the chunked one,
+// else the per-band one.  A forced choice that does not cover the grid falls
+// back the same way.
+int pick_fp64_kernel(const sht_plan *p)
+{
+  const int want = p->leg_kernel;
+  if (want == 1) return 1;
+  if (want == 2 && leg_pair_supported(p)) return 2;
+  if (want == 3 && leg_chunk_supported(p)) return 3;
+  if (leg_pair_supported(p)) return 2;
+  if (leg_chunk_supported(p)) return 3;
+  return 1;
+}
+
 int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
 {
   if (ncol <= 0) return SHT_OK;
-  if (p->leg_kernel != 1 && leg_pair_supported(p)) return launch_leg_fwd_pair(p, F, ncol, S, s);
+  switch (pick_fp64_kernel(p)) {
+  case 2: return launch_leg_fwd_pair(p, F, ncol, S, s);
+  case 3: return launch_leg_fwd_chunk(p, F, ncol, S, s);
+  default: break;
+  }
   LegArgs a{};
   a.F = F; a.S = S; a.P = p->d_P; a.poff = p->d_poff; a.rowoff = p->d_rowoff;
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;
@@ -353,7 +373,11 @@ int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *
 int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s)
 {
   if (ncol <= 0) return SHT_OK;
-  if (p->leg_kernel != 1 && leg_pair_supported(p)) return launch_leg_inv_pair(p, S, ncol, F, s);
+  switch (pick_fp64_kernel(p)) {
+  case 2: return launch_leg_inv_pair(p, S, ncol, F, s);
+  case 3: return launch_leg_inv_chunk(p, S, ncol, F, s);
+  default: break;
+  }
   LegArgs a{};
   a.Sc = S; a.Fo = F; a.P = p->d_P; a.poff = p->d_poff; a.rowoff = p->d_rowoff;
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;

@@ -18,6 +18,7 @@
 // Analysis follows space_discretization.tex:197-200 and synthesis :212-216.
 // Symmetric and antisymmetric latitude halves use Pbar(-mu) = (-1)^{n-m} Pbar(mu).
 #include "sht_internal.h"
+#include "sht_dmma.cuh"
 
 namespace sht {
 
@@ -64,25 +65,11 @@ struct V2Args {
   int N, J, JH, ncol;
 };
 
-__device__ __forceinline__ unsigned smem_u32(const void *p)
-{
-  return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-__device__ __forceinline__ void cp16(void *dst, const void *src, bool valid)
-{
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src),
-               "r"(valid ? 16 : 0));
-}
-__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::); }
-__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::); }
-
-__device__ __forceinline__ void dmma(double (&d)[2], double a, double b)
-{
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
-}
+using dmma::cp16;
+using dmma::cp_commit;
+using dmma::cp_wait0;
+using dmma::cp_wait1;
+using dmma::mma884;
 
 // Stage the Legendre rows of the pair: m_a rows at 0.., m_b rows right after.
 template <int JH>
@@ -206,8 +193,8 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) {
           const double b = gb[4 * nt * g.CS + 2 * kb];
-          dmma(acc[0][nt], a0, b);
-          dmma(acc[1][nt], a1, b);
+          mma884(acc[0][nt], a0, b);
+          mma884(acc[1][nt], a1, b);
         }
       }
       const long long rowbase = a.rowoff[m];
@@ -310,7 +297,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
           const double *brow = A + r * g.AS + (lane >> 2);
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            if (q < nnt) dmma(acc[p][q], av, brow[8 * (grp * nnt + q)]);
+            if (q < nnt) mma884(acc[p][q], av, brow[8 * (grp * nnt + q)]);
         }
       }
       const int jh = 8 * jt + (lane >> 2);

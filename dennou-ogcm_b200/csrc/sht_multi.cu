@@ -9,8 +9,9 @@
 // once as a CUDA graph (fork, per-plan stages, join) and replayed.
 //
 // The tuner times, per plan, every Legendre variant that covers the grid
-// (paired persistent FP64, chunked per-band FP64, and split precision on the
-// tensor cores when allowed) on the plan's own columns and keeps the fastest.
+// (paired persistent, latitude-chunked persistent and per-band FP64, and split
+// precision on the tensor cores when allowed) on the plan's own columns and
+// keeps the fastest.
 //
 // Workspaces belong to the batch, not to the plans, so single-plan calls made
 // between runs cannot move memory that a captured graph refers to.
@@ -135,13 +136,12 @@ int enqueue_step(sht_multi *m, int what, cudaStream_t origin)
   return SHT_OK;
 }
 
-int check_split_errors(sht_multi *m)
+int check_device_errors(sht_multi *m)
 {
-  for (Group &g : m->groups)
-    if (g.precision == SHT_PREC_SPLIT) {
-      int rc = split_error_status(g.plan);
-      if (rc) return rc;
-    }
+  for (Group &g : m->groups) {
+    int rc = device_error_status(g.plan);
+    if (rc) return rc;
+  }
   return SHT_OK;
 }
 
@@ -157,7 +157,7 @@ int time_group(Group &g, int reps, float *ms)
   } else {
     rc = group_step(g, SHT_MULTI_ROUND_TRIP);  // warm-up (builds lazy tables)
     if (!rc && (e = cudaStreamSynchronize(p->stream)) != cudaSuccess) rc = cuda_fail(e, "tuner warm-up");
-    if (!rc && g.precision == SHT_PREC_SPLIT) rc = split_error_status(p);
+    if (!rc) rc = device_error_status(p);
     if (!rc) cudaEventRecord(a, p->stream);
     for (int r = 0; r < reps && !rc; ++r) rc = group_step(g, SHT_MULTI_ROUND_TRIP);
     if (!rc) {
@@ -180,6 +180,7 @@ int tune_group(Group &g, bool allow_split)
   struct Cand { int precision, leg_kernel; };
   std::vector<Cand> cands;
   if (leg_pair_supported(g.plan)) cands.push_back({SHT_PREC_FP64, 2});
+  if (leg_chunk_supported(g.plan)) cands.push_back({SHT_PREC_FP64, 3});
   cands.push_back({SHT_PREC_FP64, 1});
   if (allow_split && split_supported(g.plan)) cands.push_back({SHT_PREC_SPLIT, 0});
   float best = 0.f;
@@ -259,7 +260,7 @@ int build(sht_multi *m, int flags)
   // one eager step: builds every lazily created table before capture
   if ((rc = enqueue_step(m, SHT_MULTI_ROUND_TRIP, m->stream))) return rc;
   if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "multi warm-up");
-  if ((rc = check_split_errors(m))) return rc;
+  if ((rc = check_device_errors(m))) return rc;
 
   // Capture each step kind: the graph is kept for replay unless the batch
   // runs stage by stage, and the capture counts the kernels of one step.
@@ -377,7 +378,7 @@ int sht_multi_synchronize(sht_multi *m)
   DevGuard g(m->device);
   cudaError_t e = cudaStreamSynchronize(m->run_stream);
   if (e != cudaSuccess) return cuda_fail(e, "multi synchronize");
-  return check_split_errors(m);
+  return check_device_errors(m);
 }
 
 int sht_multi_groups(const sht_multi *m, int *ngroups)

@@ -94,6 +94,24 @@ __device__ __forceinline__ void mbar_init(uint64_t *mbar, uint32_t count)
 }
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::); }
 
+// One thread announces `bytes` of asynchronous copies on the barrier and
+// arrives (release: shared-memory stores made before it are visible to the
+// threads that wait on the phase).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes)
+{
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(mbar)), "r"(bytes) : "memory");
+}
+
+// Bulk copy global -> shared of `bytes` (a multiple of 16; both addresses
+// 16-byte aligned), completing on the barrier (plain copy, no multicast).
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src, uint32_t bytes, uint64_t *mbar)
+{
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst_smem)),
+               "l"(src), "r"(bytes), "r"(smem_addr(mbar))
+               : "memory");
+}
+
 __device__ __forceinline__ uint64_t globaltimer_ns()
 {
   uint64_t t;

@@ -106,9 +106,10 @@ SHT_API int sht_set_precision(sht_plan *plan, int mode);
 SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
 
 /* Kernel choices (used by the autotuner and the tests; the defaults are
- * picked per grid).  SHT_OPT_LEGENDRE_KERNEL: 0 automatic, 1 per-band chunked
- * kernel (any grid), 2 persistent paired-band kernel (T85 and smaller; falls
- * back to 1 where it does not fit). */
+ * picked per grid).  SHT_OPT_LEGENDRE_KERNEL: 0 automatic, 1 per-band kernel
+ * (any grid), 2 persistent paired-band kernel (T85 and smaller), 3 persistent
+ * latitude-chunked paired-band kernel (jm/2 a multiple of 16, up to T341).
+ * A choice that does not cover the grid falls back to the automatic one. */
 #define SHT_OPT_LEGENDRE_KERNEL 1
 SHT_API int sht_set_option(sht_plan *plan, int option, int value);
 SHT_API int sht_get_option(const sht_plan *plan, int option, int *value);
