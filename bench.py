@@ -50,6 +50,21 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
+def _traffic(kernel, mode, nb):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    capture of this workload (profiles/t85_roundtrip_fp64.md), FP64 path at the
+    480 field-level batch; None for any other configuration."""
+    if mode != "fp64" or nb != LEVELS * FIELDS:
+        return None
+    try:
+        with open(os.path.join(ROOT, "profiles", "t85_dram_traffic.json")) as f:
+            t = json.load(f)
+    except Exception:
+        return None
+    keys = ("k_fft_fwd", "k_fft_inv") if kernel.startswith("k_fft") else ("k_leg_fwd_pair", "k_leg_inv_pair")
+    return 1e6 * (t[keys[0]] + t[keys[1]]) / 2
+
+
 def _rel(a, b):
     a = np.asarray(a).reshape(len(a), -1)
     b = np.asarray(b).reshape(len(b), -1)
@@ -384,7 +399,9 @@ def main():
             peak = float(fp64_dmma.value)
             pk_note = "FP64 mma.sync probe measured in this run"
     roofline = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak if peak else None, "traffic": None, "peak_source": pk_note,
+                "frac": achieved / peak if peak else None, "traffic": _traffic(name, head_mode, nb),
+                "traffic_unit": "DRAM bytes per launch (mean of the forward and inverse kernel)",
+                "algorithmic_per_launch": work / 2, "peak_source": pk_note,
                 "stage_ms_per_step": {"synthesis[fft,legendre,spectral]": st["syn"],
                                       "analysis[fft,legendre,spectral]": st["ana"]},
                 "fft_roofline_frac_of_hbm": (2 * fft_bytes / ((st["syn"][0] + st["ana"][0]) * 1e-3) / 1e9)
