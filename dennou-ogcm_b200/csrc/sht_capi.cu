@@ -297,16 +297,58 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
   double *d = static_cast<double *>(p->d_io);
   double *di0 = d, *di1 = d + al(nin_each), *do0 = d + al(nin_each) * sh.nin, *do1 = do0 + al(nout_each);
   cudaStream_t s = p->stream;
-  if ((e = cudaMemcpyAsync(di0, i0, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-    return cuda_fail(e, "H2D");
-  if (sh.nin == 2 && (e = cudaMemcpyAsync(di1, i1, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-    return cuda_fail(e, "H2D");
-  rc = run_dev(p, op, di0, sh.nin == 2 ? di1 : nullptr, nb, do0, sh.nout == 2 ? do1 : nullptr);
-  if (rc) return rc;
-  if ((e = cudaMemcpyAsync(o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-    return cuda_fail(e, "D2H");
-  if (sh.nout == 2 && (e = cudaMemcpyAsync(o1, do1, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-    return cuda_fail(e, "D2H");
+  // Large transform batches run as a pipeline of chunks: the upload of chunk
+  // c+1 (copy_in), the kernels of chunk c (plan stream) and the download of
+  // chunk c-1 (copy_out) overlap, and PCIe carries both directions at once.
+  const bool per_level = op != OP_AVRLONLAT && op != OP_INTLONLAT && op != OP_YA_AVRLON && op != OP_YA_INTLON;
+  int nchunk = per_level ? nb / 48 : 1;
+  nchunk = nchunk < 1 ? 1 : (nchunk > 8 ? 8 : nchunk);
+  if (nchunk > 1 && !p->copy_in) {
+    if ((e = cudaStreamCreateWithFlags(&p->copy_in, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaStreamCreateWithFlags(&p->copy_out, cudaStreamNonBlocking)) != cudaSuccess)
+      return cuda_fail(e, "copy streams");
+    for (auto &ev : p->chunk_ev)
+      if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e, "chunk events");
+  }
+  if (nchunk == 1) {
+    if ((e = cudaMemcpyAsync(di0, i0, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_fail(e, "H2D");
+    if (sh.nin == 2 && (e = cudaMemcpyAsync(di1, i1, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_fail(e, "H2D");
+    rc = run_dev(p, op, di0, sh.nin == 2 ? di1 : nullptr, nb, do0, sh.nout == 2 ? do1 : nullptr);
+    if (rc) return rc;
+    if ((e = cudaMemcpyAsync(o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return cuda_fail(e, "D2H");
+    if (sh.nout == 2 && (e = cudaMemcpyAsync(o1, do1, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return cuda_fail(e, "D2H");
+  } else {
+    const size_t pin = nin_each / nb, pout = nout_each / nb;  // doubles per field-level
+    // the plan stream and the copy streams start after any earlier work on the plan stream
+    if ((e = cudaEventRecord(p->chunk_ev[0], s)) != cudaSuccess) return cuda_fail(e, "chunk event");
+    if ((e = cudaStreamWaitEvent(p->copy_in, p->chunk_ev[0], 0)) != cudaSuccess) return cuda_fail(e, "chunk wait");
+    for (int c = 0; c < nchunk; ++c) {
+      const int b0 = (int)((long long)nb * c / nchunk), b1 = (int)((long long)nb * (c + 1) / nchunk), n = b1 - b0;
+      cudaEvent_t ein = p->chunk_ev[2 * c], eout = p->chunk_ev[2 * c + 1];
+      if ((e = cudaMemcpyAsync(di0 + b0 * pin, i0 + b0 * pin, sizeof(double) * n * pin, cudaMemcpyHostToDevice,
+                               p->copy_in)) != cudaSuccess ||
+          (sh.nin == 2 && (e = cudaMemcpyAsync(di1 + b0 * pin, i1 + b0 * pin, sizeof(double) * n * pin,
+                                                cudaMemcpyHostToDevice, p->copy_in)) != cudaSuccess))
+        return cuda_fail(e, "H2D");
+      if ((e = cudaEventRecord(ein, p->copy_in)) != cudaSuccess || (e = cudaStreamWaitEvent(s, ein, 0)) != cudaSuccess)
+        return cuda_fail(e, "chunk event");
+      rc = run_dev(p, op, di0 + b0 * pin, sh.nin == 2 ? di1 + b0 * pin : nullptr, n, do0 + b0 * pout,
+                   sh.nout == 2 ? do1 + b0 * pout : nullptr);
+      if (rc) return rc;
+      if ((e = cudaEventRecord(eout, s)) != cudaSuccess || (e = cudaStreamWaitEvent(p->copy_out, eout, 0)) != cudaSuccess)
+        return cuda_fail(e, "chunk event");
+      if ((e = cudaMemcpyAsync(o0 + b0 * pout, do0 + b0 * pout, sizeof(double) * n * pout, cudaMemcpyDeviceToHost,
+                               p->copy_out)) != cudaSuccess ||
+          (sh.nout == 2 && (e = cudaMemcpyAsync(o1 + b0 * pout, do1 + b0 * pout, sizeof(double) * n * pout,
+                                                 cudaMemcpyDeviceToHost, p->copy_out)) != cudaSuccess))
+        return cuda_fail(e, "D2H");
+    }
+    if ((e = cudaStreamSynchronize(p->copy_out)) != cudaSuccess) return cuda_fail(e, "D2H");
+  }
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
   if ((rc = device_error_status(p))) return rc;
   finish_timing(p, !sh.out_grid);
@@ -323,6 +365,10 @@ void free_plan(sht_plan *p)
   for (auto &ev : p->timing.ev)
     if (ev) cudaEventDestroy(ev);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
+  if (p->copy_in) cudaStreamDestroy(p->copy_in);
+  if (p->copy_out) cudaStreamDestroy(p->copy_out);
+  for (auto &ev : p->chunk_ev)
+    if (ev) cudaEventDestroy(ev);
 }
 
 }  // namespace

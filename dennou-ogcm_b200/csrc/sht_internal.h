@@ -69,6 +69,10 @@ struct sht_plan_s {
   int device = 0;
   cudaStream_t stream = nullptr;      // stream used by all work of the plan
   cudaStream_t own_stream = nullptr;  // stream created by sht_init (destroyed by sht_final)
+  // host-pointer calls: copy streams and per-chunk events of the pipelined
+  // host -> device -> host path (created on first use)
+  cudaStream_t copy_in = nullptr, copy_out = nullptr;
+  cudaEvent_t chunk_ev[16] = {};
   int precision = SHT_PREC_FP64;
   int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent
 
