@@ -2,31 +2,37 @@
 //
 // Both FP64 operands of c_n = sum_jh P_n(mu_jh) G(mu_jh) are written as
 // power-of-two scaled fixed-point numbers in balanced base-256 digits:
-//     x = 2^e * sum_{s=0..6} d_s 2^{-7-8s},   d_s integers, |d_s| <= 128,
+//     x = 2^{e-7} * sum_{s=0..6} d_s 2^{-8s},   d_s integers, |d_s| <= 128,
 // with one exponent e per row of the Legendre table and one per field-level
-// column of the data.  Every digit is exact in BF16.  Every digit product is
-// an integer of at most 2^14, so the sum over up to 128 latitudes (or degrees)
-// and up to 7 digit pairs of one significance level stays below 2^24.  It is
-// therefore exact in the FP32 accumulator of tcgen05.mma kind::f16.
-// The pairs with s + t <= 6 are kept (28 MMAs per K step).  Each level lands
-// in its own TMEM accumulator.  The levels are recombined in FP64 with the
-// two exponents (the Ozaki error-free splitting, Ozaki-Ogita-Oishi-Rump,
-// Numer. Algorithms 59 (2012)).  Each operand keeps 56 bits (the digit
-// residual is below 2^-56 of its row or column maximum), and the dropped
-// products are below 2^-62.
+// column of the data.  Digit s is stored as the BF16 value d_s 2^{-8s}
+// (exact: 8 significant bits and a power-of-two scale), so the product of
+// digits s and t carries its weight 2^{-8(s+t)} by itself.  The pairs with
+// s + t <= 6 are kept (28 MMAs per K step).  Pairs of level L = s + t < 4 go
+// to accumulator L: every such product is an integer multiple of 2^{-8L} of
+// magnitude at most 2^{14-8L}, so the FP32 sum over K <= 256 of at most four
+// pairs stays an exact multiple of at most 2^{24-8L} -- exact.  Levels 4..6
+// share a fifth accumulator; its FP32 rounding is 2^{-24} of a quantity that
+// is itself about 2^{-32} of the result's scale (keeping level 3 apart as well
+// matters: merged from level 3 on, the rounding reached 3e-11 of a field's
+// maximum on cancelling sums).  The five accumulators are summed in FP64
+// (smallest first) and scaled by the two exponents (the Ozaki error-free
+// splitting, Ozaki-Ogita-Oishi-Rump, Numer. Algorithms 59 (2012)).  Each
+// operand keeps 56 bits (the digit residual is below 2^-56 of its row or column
+// maximum), and the dropped products are below 2^-62.
 //
 // Kernel organisation (one resident CTA of 256 threads per SM):
 //   * Work item = (band pair (m, N-m), 64 complex field-level columns).  The
 //     pair keeps every item about the same cost.  An item has up to four
-//     sub-items (m, parity) and each sub-item has K chunks of 32.
+//     sub-items (m, parity); the output dimension of a sub-item (degrees in
+//     the analysis, Gauss rows in the synthesis) is cut into segments of at
+//     most kSeg columns, and each segment runs its K chunks of 32.
 //   * The data digits of chunk u+1 (and its table digits) are written into
 //     the other of two shared-memory stages while the tensor core runs the
 //     asynchronous MMAs of chunk u, issued by one thread.
-//   * When a sub-item's last chunk completes, all threads read its seven
-//     TMEM levels, 16 columns at a time (the two warp halves take alternate
+//   * When a segment's last chunk completes, all threads read its five TMEM
+//     accumulators, 16 columns at a time (the two warp halves take alternate
 //     groups), and recombine them in FP64.
 //   * M = 128 data columns (re/im of 64 field-levels; TMEM lane = column).
-//     N = degrees of one parity (analysis) or Gauss rows (synthesis).
 //     A and B are K-major in the interleaved canonical layout (8-row x
 //     16-byte core matrices, LBO = 128 B along K, SBO = 512 B across row
 //     groups).
@@ -45,6 +51,8 @@ namespace sht {
 namespace {
 
 constexpr int kS = 7;                      // digits per operand
+constexpr int kAcc = 5;                    // TMEM accumulators: levels 0, 1, 2, 3 and 4..6
+constexpr int kSeg = 96;                   // output columns per segment (kAcc x kSeg <= 512 TMEM columns)
 constexpr int kKC = 32;                    // K per chunk (2 MMA K-steps of 16)
 constexpr int kM = 128;                    // data columns per CTA (64 complex)
 constexpr int kRowB = kKC * 2;             // 64 bytes per row of one digit tile
@@ -60,32 +68,35 @@ __host__ __device__ inline uint32_t canon(int row, int k)
 __device__ __forceinline__ void digits(double x, float (&d)[kS])
 {
   // x in (-1, 1): balanced digits, d0 in [-128,128], |r| <= 1/2 after each step,
-  // so |x - sum_s d_s 2^{-7-8s}| <= 2^{-7-8 kS}
+  // so |x - 2^-7 sum_s d_s 2^{-8s}| <= 2^{-7-8 kS}; digit s is returned as d_s 2^{-8s}
   double v = x * 128.0;
 #pragma unroll
   for (int s = 0; s < kS; ++s) {
     const double q = rint(v);
-    d[s] = (float)q;
+    d[s] = ldexpf((float)q, -8 * s);
     v = (v - q) * 256.0;
   }
 }
 
-// The same digits as BF16 bit patterns without conversion instructions:
-// adding 1.5*2^52 rounds |v| < 2^51 to the nearest integer, which lands in the
-// low word; an integer d with |d| <= 128 becomes an exact FP32 value through
-// 1.5*2^23 + d, whose top 16 bits are its BF16 encoding.
+// The same scaled digits as BF16 bit patterns without conversion
+// instructions: adding 1.5*2^52 rounds |v| < 2^51 to the nearest integer,
+// which lands in the low word; an integer d with |d| <= 128 becomes an exact
+// FP32 value through 1.5*2^23 + d, the scale 2^{-8s} is an exact multiply, and
+// the top 16 bits of the FP32 value are its BF16 encoding.
 __device__ __forceinline__ void digits_bf16(double x, unsigned short (&h)[kS])
 {
   const double M52 = 6755399441055744.0;  // 1.5 * 2^52
   double v = x * 128.0;
+  float scale = 1.0f;
 #pragma unroll
   for (int s = 0; s < kS; ++s) {
     const double t = v + M52;
     const int di = __double2loint(t);
     const double q = t - M52;
     v = (v - q) * 256.0;
-    const float f = __int_as_float(0x4B400000 + di) - 12582912.0f;
+    const float f = (__int_as_float(0x4B400000 + di) - 12582912.0f) * scale;
     h[s] = (unsigned short)(__float_as_uint(f) >> 16);
+    scale *= (1.0f / 256.0f);
   }
 }
 
@@ -178,31 +189,37 @@ struct TcArgs {
   const int *teoff;   // analysis: row-exponent offsets
   int N, J, JH, ncol;
   int ntiles, nitems, per_cta;
-  int npad_max;       // TMEM columns per level
+  int npad_max;       // TMEM columns per accumulator (largest segment)
+  int npad_max_table; // rows of one synthesis digit tile (latitudes, padded)
   int *err;
 };
 
-// Sub-item bookkeeping shared by both directions.
+// Segment bookkeeping shared by both directions: sub-item (m, parity p) and
+// the segment [row0, row0 + npad) of its output dimension.
 struct Sub {
-  int m, p, Rp, npad, nch, slot;
+  int m, p, Rp, nrow, seg, nseg, row0, npad, nch, slot;
 };
 
 template <bool INV>
-__device__ __forceinline__ Sub make_sub(const TcArgs &a, int m, int p, int q)
+__device__ __forceinline__ Sub make_sub(const TcArgs &a, int m, int p, int seg, int q)
 {
   Sub s;
   s.m = m;
   s.p = p;
   s.Rp = rows_of_parity(a.N, m, p);
-  s.npad = INV ? a.npad_max : round_up(s.Rp, 16);
+  s.nrow = INV ? a.JH : s.Rp;  // output rows of the sub-item
+  s.nseg = (s.nrow + kSeg - 1) / kSeg;
+  s.seg = seg;
+  s.row0 = seg * kSeg;
+  s.npad = round_up(min(kSeg, s.nrow - s.row0), 16);
   s.nch = INV ? (s.Rp + kKC - 1) / kKC : (a.JH + kKC - 1) / kKC;
   s.slot = q & 3;
   return s;
 }
 
-// Unit iterator: (item, sub-item, chunk) in order, uniform across the CTA.
+// Unit iterator: (item, sub-item, segment, chunk) in order, uniform across the CTA.
 struct Cursor {
-  int it, sub, h, q;  // item, sub-item index within the item, chunk, running sub-item count
+  int it, sub, seg, h, q;  // item, sub-item within the item, segment, chunk, running sub-item count
 };
 
 template <bool INV>
@@ -210,7 +227,7 @@ __device__ __forceinline__ void cursor_sub(const TcArgs &a, const Cursor &c, Sub
 {
   const int2 pr = a.pairs[c.it / a.ntiles];
   const int m = (c.sub < 2) ? pr.x : pr.y;
-  out = make_sub<INV>(a, m, c.sub & 1, c.q);
+  out = make_sub<INV>(a, m, c.sub & 1, c.seg, c.q);
 }
 
 template <bool INV>
@@ -220,6 +237,8 @@ __device__ __forceinline__ void cursor_next(const TcArgs &a, Cursor &c)
   cursor_sub<INV>(a, c, s);
   if (++c.h < s.nch) return;
   c.h = 0;
+  if (++c.seg < s.nseg) return;
+  c.seg = 0;
   ++c.q;
   const int2 pr = a.pairs[c.it / a.ntiles];
   const int nsub = (pr.y >= 0) ? 4 : 2;
@@ -228,7 +247,9 @@ __device__ __forceinline__ void cursor_next(const TcArgs &a, Cursor &c)
   ++c.it;
 }
 
-// Issue the 28 digit-pair MMAs of one K chunk into D_L = tbase + L*dstride.
+// Issue the 28 digit-pair MMAs of one K chunk; level L = s + t goes to
+// accumulator min(L, kAcc - 1) at tbase + acc*dstride.  The first product into each
+// accumulator in the segment's first chunk overwrites it.
 __device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_t a_base, uint32_t b_base, int npad,
                                             bool first_chunk)
 {
@@ -237,6 +258,7 @@ __device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_
   const uint32_t b_tile = npad * kRowB;  // bytes per digit tile of B
 #pragma unroll
   for (int L = 0; L < kS; ++L) {
+    const int d = L < kAcc - 1 ? L : kAcc - 1;
 #pragma unroll
     for (int s = 0; s <= L; ++s) {
       const int t = L - s;
@@ -244,8 +266,8 @@ __device__ __forceinline__ void issue_chunk(uint32_t tbase, int dstride, uint32_
       for (int ks = 0; ks < kKC / 16; ++ks) {
         const uint64_t ad = tc::smem_desc(a_base + s * a_tile + ks * 256, 128, 512);
         const uint64_t bd = tc::smem_desc(b_base + t * b_tile + ks * 256, 128, 512);
-        const uint32_t acc = (first_chunk && s == 0 && ks == 0) ? 0u : 1u;
-        tc::mma_bf16(tbase + (uint32_t)(L * dstride), ad, bd, idesc, acc);
+        const uint32_t acc = (first_chunk && s == 0 && ks == 0 && L == d) ? 0u : 1u;
+        tc::mma_bf16(tbase + (uint32_t)(d * dstride), ad, bd, idesc, acc);
       }
     }
   }
@@ -372,11 +394,17 @@ __device__ void prepare(const TcArgs &a, const Sub &s, int h, int col0, const Sm
   }
   // B: the table chunk (kS tiles of npad rows x 32 k), contiguous; copied
   // asynchronously (all 16-byte pieces in flight at once), completed below
+  // the segment's rows [row0, row0 + npad) of each digit tile are one run of
+  // npad * 64 bytes (row0 is a multiple of 8, whole core-matrix groups)
   const int mp = s.m * 2 + s.p;
-  const char *src = reinterpret_cast<const char *>(a.tab + a.toff[mp]) + (size_t)h * kS * s.npad * kRowB;
-  const int n16 = kS * s.npad * kRowB / 16;
-  for (int q = tid; q < n16; q += kThreads)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(sm.B[st] + 16 * q)), "l"(src + 16 * q));
+  const int tile_rows = INV ? a.npad_max_table : round_up(s.Rp, 16);
+  const char *src = reinterpret_cast<const char *>(a.tab + a.toff[mp]) + ((size_t)h * kS * tile_rows + s.row0) * kRowB;
+  const int per_tile = s.npad * kRowB / 16;  // 16-byte pieces per digit tile
+  for (int q = tid; q < kS * per_tile; q += kThreads) {
+    const int t = q / per_tile, r = q - t * per_tile;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(tc::smem_addr(sm.B[st] + (size_t)t * s.npad * kRowB + 16 * r)),
+                 "l"(src + (size_t)t * tile_rows * kRowB + 16 * r));
+  }
   asm volatile("cp.async.commit_group;\n" ::);
 }
 
@@ -397,12 +425,12 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
 #pragma unroll
     for (int i = 0; i < 16; ++i) acc[i] = 0.0;
 #pragma unroll
-    for (int L = kS - 1; L >= 0; --L) {
+    for (int d = kAcc - 1; d >= 0; --d) {  // smallest first
       uint32_t r[16];
-      tc::tmem_ld16(lane_base + (uint32_t)(L * a.npad_max + 16 * g), r);
+      tc::tmem_ld16(lane_base + (uint32_t)(d * a.npad_max + 16 * g), r);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int i = 0; i < 16; ++i) acc[i] = acc[i] * (1.0 / 256.0) + (double)__uint_as_float(r[i]);
+      for (int i = 0; i < 16; ++i) acc[i] += (double)__uint_as_float(r[i]);
     }
     if (!valid) continue;
     if (!INV) {
@@ -410,7 +438,7 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
       const long long rowbase = a.rowoff[s.m];
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const int n = 16 * g + i;
+        const int n = s.row0 + 16 * g + i;
         if (n < s.Rp)
           reinterpret_cast<double *>(a.S + (rowbase + s.p + 2 * n) * a.ncol + b)[part] = ldexp(acc[i], e + fe[n] - 14);
       }
@@ -421,13 +449,14 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
       double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + b) * a.J) + part;
       const int JH = a.JH;
       double gev[16];
+      const int j0 = s.row0 + 16 * g;
       if (s.p == 1) {
 #pragma unroll
-        for (int i = 0; i < 16; ++i) gev[i] = (16 * g + i < JH) ? Fc[2 * (JH + 16 * g + i)] : 0.0;
+        for (int i = 0; i < 16; ++i) gev[i] = (j0 + i < JH) ? Fc[2 * (JH + j0 + i)] : 0.0;
       }
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
-        const int jh = 16 * g + i;
+        const int jh = j0 + i;
         if (jh >= JH) continue;
         const double v = ldexp(acc[i], e + ge[jh] - 14);
         if (s.p == 0) {
@@ -478,7 +507,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_split(TcArgs a)
   uint32_t ph_stage[2] = {0, 0}, ph_tmem = 0;
   bool ok = true;
 
-  Cursor cur{it0, 0, 0, 0};
+  Cursor cur{it0, 0, 0, 0, 0};
   Sub s;
   cursor_sub<INV>(a, cur, s);
   {
@@ -516,7 +545,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_split(TcArgs a)
         ph_stage[st ^ 1] ^= 1;
       }
       if (ok) {
-        if (nxt.h == 0 && (INV || sn.p == 0)) column_exponents<INV>(a, sn, ncol0, sm);
+        if (nxt.h == 0 && nxt.seg == 0 && (INV || sn.p == 0)) column_exponents<INV>(a, sn, ncol0, sm);
         prepare<INV>(a, sn, nxt.h, ncol0, sm, st ^ 1);
         prepare_done();
         tc::fence_proxy_async();
@@ -613,7 +642,7 @@ int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2
   if (ncol <= 0) return SHT_OK;
   if (!split_supported(p)) {
     set_error("split precision: this grid is not covered by the tensor-core kernel "
-              "(needs jm <= 128 with jm/2 a multiple of 16, and nm <= 125)");
+              "(needs jm <= 512 and nm <= 509, so that no exact level sums over more than 256 terms)");
     return SHT_ERR_UNSUPPORTED_SIZE;
   }
   int rc = build_split_tables(p);
@@ -621,10 +650,12 @@ int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2
   SplitTables *t = tables(p);
   TcArgs a{};
   if (inverse) {
-    a.Sc = in; a.Fo = out; a.tab = t->inv; a.toff = t->inv_off; a.texp = t->inv_exp; a.npad_max = t->inv_npad;
+    a.Sc = in; a.Fo = out; a.tab = t->inv; a.toff = t->inv_off; a.texp = t->inv_exp;
+    a.npad_max = t->inv_npad < kSeg ? t->inv_npad : kSeg;
+    a.npad_max_table = t->inv_npad;
   } else {
     a.F = in; a.S = out; a.tab = t->fwd; a.toff = t->fwd_off; a.texp = t->fwd_exp; a.teoff = t->fwd_eoff;
-    a.npad_max = t->fwd_npad_max;
+    a.npad_max = t->fwd_npad_max < kSeg ? t->fwd_npad_max : kSeg;
   }
   a.rowoff = p->d_rowoff; a.pairs = p->d_pairs;
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol; a.err = t->d_err;
@@ -647,11 +678,12 @@ int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2
 
 bool split_supported(const sht_plan *p)
 {
-  // TMEM holds the kS levels of one sub-item: kS * NPAD <= 512 columns; the
-  // accumulation over at most 128 latitudes or degrees keeps every level exact.
-  const int npmax = round_up((p->N + 3) / 2, 16);
-  const int inpad = round_up(p->JH, 16);
-  return p->JH <= 64 && npmax * kS <= 512 && inpad * kS <= 512 && split_smem(npmax > inpad ? npmax : inpad) <= 227 * 1024;
+  // TMEM holds the kAcc accumulators of one segment (kAcc * kSeg <= 512
+  // columns); the exact levels sum over at most 256 latitudes (analysis) or
+  // degrees of one parity (synthesis).
+  static_assert(kAcc * kSeg <= 512, "TMEM columns");
+  const int Rmax = (p->N + 3) / 2;
+  return p->JH <= 256 && Rmax <= 256 && split_smem(kSeg) <= 227 * 1024;
 }
 
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)

@@ -13,7 +13,7 @@ from conftest import pkg, relerr, workloads
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-11
-GRIDS = [(64, 32, 21), (128, 64, 42), (256, 128, 85)]
+GRIDS = [(64, 32, 21), (128, 64, 42), (256, 128, 85), (512, 256, 170)]
 
 
 @pytest.fixture(scope="module")
@@ -88,9 +88,30 @@ def test_split_t85_full_batch_round_trip(plan_cache):
     assert relerr(out, w) < TOL
 
 
+def test_split_t341_matches_fp64(plan_cache):
+    """T341 (segments of the output dimension, 256-term exact level sums)
+    against the FP64 GPU path and as a round trip."""
+    P, W = pkg(), workloads()
+    I, J, N = W.GRIDS["T341"]
+    gpu, _ = plan_cache(I, J, N)
+    w = W.seeded_spectra(N, 24, 2.0, seed=9)
+    g64 = gpu.xya_wa(w)
+    gpu.set_precision(P.SHT_PREC_SPLIT)
+    try:
+        g = gpu.xya_wa(w)
+        back = gpu.wa_xya(g)
+        gpu.synchronize()
+    finally:
+        gpu.set_precision(P.SHT_PREC_FP64)
+    assert relerr(g, g64) < TOL
+    assert relerr(back, w) < TOL
+
+
 def test_split_rejects_grids_it_does_not_cover(plan_cache):
+    """More than 256 half-latitudes would put more than 256 terms into an
+    exact FP32 level sum."""
     P = pkg()
-    gpu, _ = plan_cache(512, 256, 170)
+    gpu, _ = plan_cache(64, 1024, 21)
     gpu.set_precision(P.SHT_PREC_SPLIT)
     try:
         with pytest.raises(P.SpmlError) as ei:
