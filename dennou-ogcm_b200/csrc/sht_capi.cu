@@ -430,20 +430,38 @@ int sht_nm_l(int l, int *n, int *m)
   return SHT_OK;
 }
 
+int sht_plan_l_nm(const sht_plan *p, int n, int m)
+{
+  if (!live(p)) { set_error("plan is not initialised"); return 0; }
+  if (n < 0 || n > p->N || m < -n || m > n || (p->zonal && m != 0)) return 0;
+  return p->zonal ? n + 1 : n * (n + 1) + m + 1;
+}
+
+int sht_plan_nm_l(const sht_plan *p, int l, int *n, int *m)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (!n || !m || l < 1 || l > p->L) { set_error("nm_l: index out of range"); return SHT_ERR_INVALID_ARG; }
+  if (p->zonal) { *n = l - 1; *m = 0; return SHT_OK; }
+  return sht_nm_l(l, n, m);
+}
+
 int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
 {
   if (!out) { set_error("init: plan pointer is NULL"); return SHT_ERR_INVALID_ARG; }
   *out = nullptr;
-  if (nm == -1) nm = (im - 1) / 3;
+  const bool zonal = (im == 1);  // DOGCM_MODE_AXISYM: wa_zonal_module, lm = nm + 1
+  // default truncations of util/grid/DOGCM_GaussSpmVFvmGrid_mod.f90:206-209
+  if (nm == -1) nm = zonal ? (2 * jm - 1) / 3 : (im - 1) / 3;
   int lg = 0;
   while ((1 << lg) < im) ++lg;
-  if (im < 16 || im > 2048 || (1 << lg) != im) {
-    set_error("init: im must be a power of two in [16, 2048]");
+  if (!zonal && (im < 16 || im > 2048 || (1 << lg) != im)) {
+    set_error("init: im must be 1 (axisymmetric) or a power of two in [16, 2048]");
     return SHT_ERR_UNSUPPORTED_SIZE;
   }
   if (jm < 2 || (jm & 1)) { set_error("init: jm must be even and >= 2"); return SHT_ERR_UNSUPPORTED_SIZE; }
-  if (nm < 0 || im < 2 * nm + 2 || jm <= nm) {
-    set_error("init: need 0 <= nm, im >= 2 nm + 2 and jm > nm");
+  if (nm < 0 || (!zonal && im < 2 * nm + 2) || jm <= nm) {
+    set_error("init: need 0 <= nm, im >= 2 nm + 2 (unless im = 1) and jm > nm");
     return SHT_ERR_UNSUPPORTED_SIZE;
   }
   if (nm > 1023 || !(radius > 0.0) || km < 0) { set_error("init: bad nm/radius/km"); return SHT_ERR_INVALID_ARG; }
@@ -456,6 +474,7 @@ int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
   sht_plan *p = new (std::nothrow) sht_plan();
   if (!p) { set_error("init: host allocation failed"); return SHT_ERR_ALLOC; }
   p->I = im; p->J = jm; p->N = nm; p->K = km; p->JH = jm / 2; p->NC = im / 2; p->radius = radius;
+  p->zonal = zonal;
   cudaGetDevice(&p->device);
   int rc = SHT_OK;
   if ((e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking)) != cudaSuccess) rc = cuda_fail(e, "stream create");
@@ -523,8 +542,12 @@ int sht_rn(const sht_plan *p, double *rn)
   int rc = check_plan(p);
   if (rc) return rc;
   if (!rn) { set_error("rn: NULL output"); return SHT_ERR_INVALID_ARG; }
+  // p->L entries in the plan's layout: l = n(n+1)+m, or l = n for a zonal plan
   for (int n = 0; n <= p->N; ++n)
-    for (int m = -n; m <= n; ++m) rn[n * (n + 1) + m] = -(double)n * (n + 1);
+    for (int m = -n; m <= n; ++m) {
+      if (p->zonal && m != 0) continue;
+      rn[p->zonal ? n : n * (n + 1) + m] = -(double)n * (n + 1);
+    }
   return SHT_OK;
 }
 

@@ -377,6 +377,29 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
   cp_async_wait<0>();
 }
 
+// Zonal plans (im = 1, the wa_zonal_module transform): the longitude
+// transform of a single point is the identity, so only the row scale remains,
+// G^0_j = s_j q_j (forward) and q_j = s_j Re G^0_j (inverse).
+__global__ void __launch_bounds__(256) k_zonal_fwd(FftArgs a)
+{
+  const long long total = (long long)a.ncol * a.J;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(k / a.J), j = (int)(k - (long long)col * a.J);
+    const double *src = a.gcol ? a.gcol[col] : (col < a.nsplit) ? a.g0 + (long long)col * a.J : a.g1 + (long long)(col - a.nsplit) * a.J;
+    a.F[(long long)(a.colF0 + col) * a.J + j] = make_double2(src[j] * __ldg(a.rowscale + j), 0.0);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_zonal_inv(FftArgs a)
+{
+  const long long total = (long long)a.ncol * a.J;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
+    const int col = (int)(k / a.J), j = (int)(k - (long long)col * a.J);
+    double *dst = a.ocol ? a.ocol[col] : (col < a.nsplit) ? a.o0 + (long long)col * a.J : a.o1 + (long long)(col - a.nsplit) * a.J;
+    dst[j] = a.Fc[(long long)(a.colF0 + col) * a.J + j].x * __ldg(a.rowscale + j);
+  }
+}
+
 namespace {
 constexpr int kFftThreads = 128;
 
@@ -429,6 +452,17 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s
 
 int dispatch(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s)
 {
+  if (p->zonal) {
+    const long long total = (long long)args.ncol * p->J;
+    if (total <= 0) return SHT_OK;
+    long long g = (total + 255) / 256;
+    if (g > 148 * 8) g = 148 * 8;
+    if (inverse) k_zonal_inv<<<(unsigned)g, 256, 0, s>>>(args);
+    else k_zonal_fwd<<<(unsigned)g, 256, 0, s>>>(args);
+    count_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_zonal_inv" : "k_zonal_fwd");
+  }
   switch (p->NC) {
   case 8: return run_fft<2, 1>(inverse, p, args, s);
   case 16: return run_fft<2, 2>(inverse, p, args, s);

@@ -73,6 +73,8 @@ struct sht_plan_s {
   // host -> device -> host path (created on first use)
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t chunk_ev[16] = {};
+  bool zonal = false;  // im = 1: the axisymmetric (m = 0) transform of wa_zonal_module, lm = nm + 1
+  int M = 0;           // orders transformed: N + 1, or 1 for a zonal plan
   int precision = SHT_PREC_FP64;
   int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent
 

@@ -356,7 +356,7 @@ int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;
   const int R0 = p->N + 2, ng0 = ((R0 + 1) / 2 + 15) / 16 + (R0 / 2 + 15) / 16;
   const int maxu = (ng0 + kWarps - 1) / kWarps;
-  dim3 grid((ncol + kCT - 1) / kCT, p->N + 1);
+  dim3 grid((ncol + kCT - 1) / kCT, p->M);
   // the red buffer (8 x 32 x 16 doubles) fits inside the P staging area
   static_assert(kWarps * 16 * kPS >= kWarps * 32 * 16, "reduction buffer must fit in the P staging area");
   const size_t smem = fwd_smem();
@@ -383,7 +383,7 @@ int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol;
   const int ngj = (p->JH + 15) / 16;
   const int maxu = (ngj + kWarps - 1) / kWarps;
-  dim3 grid((ncol + kCT - 1) / kCT, p->N + 1);
+  dim3 grid((ncol + kCT - 1) / kCT, p->M);
   const size_t smem = inv_smem();
   switch (maxu) {
   case 1: return launch(k_leg_inv_dmma<1>, grid, smem, s, a, "k_leg_inv_dmma");

@@ -96,11 +96,12 @@ static int dalloc(T **ptr, size_t count)
 int build_tables(sht_plan *p)
 {
   const int I = p->I, J = p->J, N = p->N, JH = p->JH, NC = p->NC;
-  int lg = ilog2_exact(NC);
+  int lg = p->zonal ? 0 : ilog2_exact(NC);
   p->fb = lg / 2;
   p->fa = lg - p->fb;
   p->R = (long long)(N + 1) * (N + 4) / 2;
-  p->L = (N + 1) * (N + 1);
+  p->M = p->zonal ? 1 : N + 1;
+  p->L = p->zonal ? N + 1 : (N + 1) * (N + 1);
   int rc;
   // --- Gauss nodes and weights on the device
   if ((rc = dalloc(&p->d_mu, J)) || (rc = dalloc(&p->d_wgt, J))) return rc;
@@ -176,10 +177,12 @@ int build_tables(sht_plan *p)
   if ((e = cudaMemcpyAsync(p->d_rowscale, rs.data(), sizeof(double) * rs.size(), cudaMemcpyHostToDevice, p->stream)) != cudaSuccess)
     return cuda_fail(e, "rowscale upload");
 
-  // --- Laplacian eigenvalues rn(l,1) = -n(n+1)
+  // --- Laplacian eigenvalues rn(l,1) = -n(n+1) (zonal layout: l = n)
   std::vector<double> rn(p->L);
   for (int n = 0; n <= N; ++n)
-    for (int m = -n; m <= n; ++m) rn[n * (n + 1) + m] = -(double)n * (n + 1);
+    for (int m = -n; m <= n; ++m)
+      if (!p->zonal) rn[n * (n + 1) + m] = -(double)n * (n + 1);
+      else if (m == 0) rn[n] = -(double)n * (n + 1);
   if ((rc = dalloc(&p->d_rn, p->L))) return rc;
   if ((e = cudaMemcpyAsync(p->d_rn, rn.data(), sizeof(double) * p->L, cudaMemcpyHostToDevice, p->stream)) != cudaSuccess)
     return cuda_fail(e, "rn upload");
@@ -187,14 +190,18 @@ int build_tables(sht_plan *p)
   std::vector<int2> tiles;
   for (int n = 0; n <= N + 1; ++n) {
     if (n == N + 1) p->n_pack_tiles = (int)tiles.size();
-    const int mmax = n < N ? n : N;
+    const int mmax = p->zonal ? 0 : (n < N ? n : N);
     for (int m0 = 0; m0 <= mmax; m0 += 32) tiles.push_back(make_int2(n, m0));
   }
   p->n_spec_tiles = (int)tiles.size();
   // --- band pairs (m, N-m) with N+4 degrees each, plus the middle band of even N
   std::vector<int2> pairs;
-  for (int m = 0; m < N - m; ++m) pairs.push_back(make_int2(m, N - m));
-  if (N % 2 == 0) pairs.push_back(make_int2(N / 2, -1));
+  if (p->zonal) {
+    pairs.push_back(make_int2(0, -1));  // the m = 0 band alone
+  } else {
+    for (int m = 0; m < N - m; ++m) pairs.push_back(make_int2(m, N - m));
+    if (N % 2 == 0) pairs.push_back(make_int2(N / 2, -1));
+  }
   p->n_pairs = (int)pairs.size();
   if ((rc = dalloc(&p->d_pairs, pairs.size()))) return rc;
   if ((e = cudaMemcpyAsync(p->d_pairs, pairs.data(), sizeof(int2) * pairs.size(), cudaMemcpyHostToDevice, p->stream)) != cudaSuccess)

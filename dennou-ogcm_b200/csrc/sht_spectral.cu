@@ -45,7 +45,15 @@ struct SpecArgs {
   const int2 *tiles;      // (n, m0) per tile
   double *const *ocol;        // optional per-field-level pack destinations
   const double *const *icol;  // optional per-field-level unpack sources
+  int M;                      // orders present: N + 1, or 1 for a zonal plan
+  int zonal;                  // SPML index l = n (wa_zonal_module) instead of n(n+1) +- m
 };
+
+// 0-based SPML index of (n, m), cos (sn = 0) or sin (sn = 1) part
+__device__ __forceinline__ long long spml_l(const SpecArgs &a, int n, int m, int sn)
+{
+  return a.zonal ? (long long)n : (long long)n * (n + 1) + (sn ? -m : m);
+}
 
 __device__ __forceinline__ double eps_at(const SpecArgs &a, int m, int n)
 {
@@ -70,7 +78,7 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   for (int mi = warp; mi < kMC; mi += 8) {
     const int m = m0 + mi;
     double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
-    if (m <= n && b < a.nb) {
+    if (m <= n && m < a.M && b < a.nb) {
       const long long base = (long long)(__ldg(a.rowoff + m) + (n - m)) * a.ncolS;
       auto ld = [&](int dn, int set) -> double2 {
         const int nn = n + dn;
@@ -106,15 +114,14 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   __syncthreads();
   // write runs w[b][n(n+1) + m] and w[b][n(n+1) - m]
   const int mi = lane, m = m0 + mi;
-  const long long lc = (long long)n * (n + 1);
   for (int bi = warp; bi < kBC; bi += 8) {
     const int bb = b0 + bi;
-    if (bb >= a.nb || m > n) continue;
+    if (bb >= a.nb || m > n || m >= a.M) continue;
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
       double *w = (o == 0 && a.ocol) ? a.ocol[bb] : ((o == 0) ? a.o0 : a.o1) + (long long)bb * a.L;
-      w[lc + m] = out[o][0][mi][bi];
-      if (m > 0) w[lc - m] = out[o][1][mi][bi];
+      w[spml_l(a, n, m, 0)] = out[o][0][mi][bi];
+      if (m > 0) w[spml_l(a, n, m, 1)] = out[o][1][mi][bi];
     }
   }
 }
@@ -162,10 +169,9 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
     val[i] = 0.0;
     if (!unpack_needs<OP>(in, dn)) continue;
     const int nn = n + dn, bb = b0 + 8 * (i % (kBC / 8)) + warp;
-    if (nn >= 0 && nn <= a.N && m <= nn && bb < a.nb && !(sn && m == 0)) {
+    if (nn >= 0 && nn <= a.N && m <= nn && m < a.M && bb < a.nb && !(sn && m == 0)) {
       const double *w = (in == 0 && a.icol) ? a.icol[bb] : ((in == 0) ? a.w0 : a.w1) + (long long)bb * a.L;
-      const long long l = (long long)nn * (nn + 1) + (sn ? -m : m);
-      val[i] = __ldg(w + l);
+      val[i] = __ldg(w + spml_l(a, nn, m, sn));
     }
   }
 #pragma unroll
@@ -179,7 +185,7 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
   if (b >= a.nb) return;
   for (int mi = warp; mi < kMC; mi += 8) {
     const int m = m0 + mi;
-    if (m > n || m > a.N) continue;
+    if (m > n || m > a.N || m >= a.M) continue;
     const double s = (m == 0) ? 1.0 : kRSqrt2;
     auto coef = [&](int in, int dn) -> double2 {
       const int run = in * 6 + (dn + 1) * 2;
@@ -282,6 +288,7 @@ int launch_pack(const sht_plan *p, int op, const double2 *S, int ncolS, int nb, 
   a.S = S; a.ncolS = ncolS; a.o0 = w0; a.o1 = w1 ? w1 : w0;
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
   a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
+  a.M = p->M; a.zonal = p->zonal ? 1 : 0;
   dim3 grid(p->n_pack_tiles, (nb + kBC - 1) / kBC);
   switch (op) {
   case PACK_PLAIN: k_pack<PACK_PLAIN><<<grid, 256, 0, s>>>(a); break;
@@ -305,6 +312,7 @@ int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1,
   a.So = S; a.ncolS = ncolS; a.w0 = w0; a.w1 = w1 ? w1 : w0;
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
   a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
+  a.M = p->M; a.zonal = p->zonal ? 1 : 0;
   dim3 grid(p->n_spec_tiles, (nb + kBC - 1) / kBC);
   const size_t one = sizeof(double) * kMC * (kBC + 1);  // one staged run
   cudaError_t e = cudaSuccess;

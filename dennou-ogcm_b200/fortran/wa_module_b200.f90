@@ -53,6 +53,11 @@ module wa_module_b200
       import :: c_int, c_ptr
       type(c_ptr), value :: plan
     end function sht_final
+    integer(c_int) function sht_dims(plan, im, jm, nm, lm) bind(C, name='sht_dims')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan
+      integer(c_int), intent(out) :: im, jm, nm, lm
+    end function sht_dims
     integer(c_int) function sht_grid_info(plan, x_lon, y_lat, x_w, y_w) bind(C, name='sht_grid_info')
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: plan
@@ -196,11 +201,15 @@ contains
     real(DP), intent(in), optional :: radius
     real(DP) :: a
     integer :: i, j
+    integer(c_int) :: ci, cj, cn, cl
     a = 1.0_DP
     if (present(radius)) a = radius
-    nm = n_in; im = i_in; jm = j_in; lm = (nm + 1)**2
-    call check(sht_init(int(im, c_int), int(jm, c_int), int(k_in, c_int), int(nm, c_int), &
+    call check(sht_init(int(i_in, c_int), int(j_in, c_int), int(k_in, c_int), int(n_in, c_int), &
          real(a, c_double), plan), 'wa_Initial')
+    ! the plan fixes nm (nm = -1 selects the default) and lm: (nm+1)**2, or
+    ! nm+1 for the axisymmetric model (im = 1, SpmlUtil_mod.f90:210-214)
+    call check(sht_dims(plan, ci, cj, cn, cl), 'wa_Initial')
+    im = ci; jm = cj; nm = cn; lm = cl
     allocate(x_Lon(0:im-1), y_Lat(jm), x_Lon_Weight(0:im-1), y_Lat_Weight(jm))
     allocate(xy_Lon(0:im-1, jm), xy_Lat(0:im-1, jm), rn(lm, 2))
     call check(sht_grid_info(plan, x_Lon, y_Lat, x_Lon_Weight, y_Lat_Weight), 'wa_Initial')

@@ -96,6 +96,8 @@ def load_library(path: str | None = None):
     for suf in ("", "_dev"):
         getattr(lib, "sht_wa_diffuse" + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
     lib.sht_roundtrip_diffuse_dev.argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
+    lib.sht_plan_l_nm.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
+    lib.sht_plan_nm_l.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_create.argtypes = [ctypes.POINTER(_VP)]
     lib.sht_multi_add.argtypes = [_VP, _VP, ctypes.c_int, _VP, _VP, ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_build.argtypes = [_VP, ctypes.c_int]
@@ -185,6 +187,21 @@ class SpmlUtil:
         return {"x_Lon": xl, "y_Lat": yl, "x_Lon_Weight": xw, "y_Lat_Weight": yw,
                 "xy_Lon": np.broadcast_to(xl[None, :], (jm, im)).copy(),
                 "xy_Lat": np.broadcast_to(yl[:, None], (jm, im)).copy()}
+
+    @property
+    def zonal(self) -> bool:
+        """True for an axisymmetric plan (iMax = 1: wa_zonal_module, lm = nm + 1)."""
+        return self.im == 1
+
+    def l_nm(self, n: int, m: int) -> int:
+        """1-based spectral index of (n, m) in this plan's layout (0 if absent)."""
+        return int(load_library().sht_plan_l_nm(self._h, int(n), int(m)))
+
+    def nm_l(self, l: int):
+        """(n, m) of the 1-based spectral index l in this plan's layout."""
+        n, m = ctypes.c_int(), ctypes.c_int()
+        _check(load_library().sht_plan_nm_l(self._h, int(l), ctypes.byref(n), ctypes.byref(m)), "nm_l")
+        return n.value, m.value
 
     @property
     def rn(self):
@@ -340,6 +357,9 @@ class SpmlUtil:
 
     def w_LaplaInv_w(self, w):
         return self._run("sht_wa_laplainv_wa", [w], "spec")
+
+    wa_Lapla_wa = w_Lapla_w
+    wa_LaplaInv_wa = w_LaplaInv_w
 
     def AvrLonLat_xy(self, xy):
         return self._run("sht_avrlonlat_xya", [xy], "avr")

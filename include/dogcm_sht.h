@@ -70,12 +70,15 @@ SHT_API const char *sht_last_error(void);
 
 /* SpmlUtil_Init(iMax, jMax, kMax, nMax, tMax, RPlanet, np)
  * (SpmlUtil_mod.f90:192-241; wa_Initial at :218-223).
- * im: longitudes (a power of two, 8..2048), jm: Gauss latitudes (even),
- * km: levels (the default batch; informational), nm: triangular truncation
- * (nm = -1 selects (im-1)/3 as in util/grid/DOGCM_GaussSpmVFvmGrid_mod.f90:209),
+ * im: longitudes (a power of two, 16..2048), or 1 for the axisymmetric model
+ * (DOGCM_MODE_AXISYM, SpmlUtil_mod.f90:30-35,210-211: SPMODEL
+ * wa_zonal_module, only the m = 0 modes, lm = nm + 1 with wa(n+1) = a_n^0);
+ * jm: Gauss latitudes (even); km: levels (the default batch; informational);
+ * nm: triangular truncation (nm = -1 selects (im-1)/3, or (2 jm - 1)/3 when
+ * im = 1, as util/grid/DOGCM_GaussSpmVFvmGrid_mod.f90:206-209 does);
  * radius: planetary radius (Radius in SpmlUtil_mod).  Requires
- * im >= 2 nm + 2 and jm > nm.  Builds the Gauss nodes and weights and the
- * associated-Legendre table on the device in FP64. */
+ * im >= 2 nm + 2 (unless im = 1) and jm > nm.  Builds the Gauss nodes and
+ * weights and the associated-Legendre table on the device in FP64. */
 SHT_API int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **plan);
 
 /* SpmlUtil_Final (SpmlUtil_mod.f90:243-256).  Frees the plan. */
@@ -96,6 +99,11 @@ SHT_API int sht_grid_info(const sht_plan *plan, double *x_lon, double *y_lat,
 /* l_nm / nm_l (re-exported at SpmlUtil_mod.f90:120): 1-based spectral index. */
 SHT_API int sht_l_nm(int n, int m);
 SHT_API int sht_nm_l(int l, int *n, int *m);
+
+/* The same maps for the plan's layout (the axisymmetric layout is l = n + 1,
+ * m = 0); sht_plan_l_nm returns 0 for a pair the plan does not hold. */
+SHT_API int sht_plan_l_nm(const sht_plan *plan, int n, int m);
+SHT_API int sht_plan_nm_l(const sht_plan *plan, int l, int *n, int *m);
 
 /* rn(:,1) (SpmlUtil_mod.f90:135): Laplacian eigenvalue -n(n+1) per l. */
 SHT_API int sht_rn(const sht_plan *plan, double *rn);

@@ -42,7 +42,7 @@ def test_index_maps_and_status_text():
 
 
 @pytest.mark.parametrize("args", [(63, 32, 1, 21), (64, 31, 1, 21), (64, 32, 1, 40), (4096, 512, 1, 100),
-                                  (64, 16, 1, 21)])
+                                  (64, 16, 1, 21), (2, 64, 1, 0), (1, 63, 1, 21), (1, 64, 1, 64)])
 def test_init_rejects_unsupported_grids(args):
     """Sizes are validated on the host before any device work (status 2)."""
     lib = pkg().load_library()
