@@ -9,12 +9,17 @@
 // A real row of I = 2 NC points is packed as NC complex points, transformed by
 // a four-step FFT with NC = R1 R2 (R1-point DFTs in registers, a twiddle, a
 // transpose through shared memory, R2-point DFTs in registers), and unpacked
-// with the usual half-length real-FFT identity.  Each thread block owns JT
-// consecutive latitude rows of one field-level and T = R2 threads per row;
-// its Fourier output is staged in shared memory and written as JT-long
-// contiguous runs of F[m][col][j] (coalesced), which is the layout the
-// Legendre contraction reads.  Shared-memory strides are padded so that each
-// 8-lane phase of a 16-byte access touches eight distinct bank groups.
+// with the usual half-length real-FFT identity.  Each tile of a thread block
+// holds JT/2 mirrored pairs of Gauss rows of one field-level (north row
+// JH + jh and south row JH - 1 - jh for jh0 <= jh < jh0 + JT/2), T = R2
+// threads per row.  The Fourier array carries the equatorial symmetry that
+// the Legendre contraction uses: F[m][col][jh] = G(north) + G(south) and
+// F[m][col][JH + jh] = G(north) - G(south) in the analysis (Gs, Ga); in the
+// synthesis the contraction writes the even- and odd-degree sums E and O
+// there, and the inverse transform forms G(north) = E + O, G(south) = E - O.
+// The output is staged in shared memory and written as runs of JT/2 rows.
+// Shared-memory strides are padded so that each 8-lane phase of a 16-byte
+// access touches eight distinct bank groups.
 #include "sht_internal.h"
 
 namespace sht {
@@ -116,7 +121,7 @@ struct FftArgs {
   int ncolF, colF0;
   const double *rowscale;
   const double2 *tw, *twI;
-  int I, J, N;
+  int I, J, JH, N;
   const double *const *gcol;  // optional per-column grid sources (forward)
   double *const *ocol;        // optional per-column grid destinations (inverse)
 };
@@ -177,22 +182,24 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
   double2 *stw = smem_all, *stwI = smem_all + NC, *sm = smem_all + 2 * NC;
   load_twiddles<T, NC, NT>(a, stw, stwI);
 
+  constexpr int JTh = JT / 2;  // mirrored row pairs per tile
   const int tid = threadIdx.x, r = tid / T, u = tid % T;
-  const int ntile = (a.J + JT - 1) / JT;
+  const int ntile = (a.JH + JTh - 1) / JTh;
   const long long ntot = (long long)a.ncol * ntile;
   const long long IJ = (long long)a.I * a.J;
   const long long mstride = (long long)a.ncolF * a.J;
 
   auto issue = [&](long long t, double2 *buf) {
-    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT;
+    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
     const double *gb = a.gcol ? a.gcol[col]
                      : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
-    const double2 *src = reinterpret_cast<const double2 *>(gb + (long long)j0 * a.I);
-    const int nrows = min(JT, a.J - j0);
+    const double2 *src = reinterpret_cast<const double2 *>(gb);
 #pragma unroll 4
     for (int q = tid; q < JT * NC; q += NT) {
       const int rr = q / NC, c = q - rr * NC;
-      if (rr < nrows) cp_async16(buf + rr * NCp + c, src + (long long)rr * NC + c, true);
+      const int jh = h0 + (rr % JTh);
+      const int j = rr < JTh ? a.JH + jh : a.JH - 1 - jh;
+      if (jh < a.JH) cp_async16(buf + rr * NCp + c, src + (long long)j * NC + c, true);
     }
   };
 
@@ -206,8 +213,9 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
     cp_async_wait<1>();
     __syncthreads();
 
-    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT, j = j0 + r;
-    const bool valid = j < a.J;
+    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
+    const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
+    const bool valid = jh < a.JH;
     // pass A: R1-point DFTs over elements strided by R2
     double2 v[R1];
 #pragma unroll
@@ -264,12 +272,16 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
     }
     __syncthreads();
 
-    // Fourier runs F[m][col][j0 .. j0+JT)
-    const int nrows = min(JT, a.J - j0);
-    double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + j0;
-    for (int idx = tid; idx < (a.N + 1) * JT; idx += NT) {
-      const int m = idx / JT, rr = idx - m * JT;
-      if (rr < nrows) Fb[m * mstride + rr] = cur[m * JTp + rr];
+    // runs Gs = north + south at F[m][col][jh], Ga = north - south at F[m][col][JH + jh]
+    const int nh = min(JTh, a.JH - h0);
+    double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + h0;
+    for (int idx = tid; idx < (a.N + 1) * JTh; idx += NT) {
+      const int m = idx / JTh, i = idx - m * JTh;
+      if (i < nh) {
+        const double2 gn = cur[m * JTp + i], gs = cur[m * JTp + JTh + i];
+        Fb[m * mstride + i] = make_double2(gn.x + gs.x, gn.y + gs.y);
+        Fb[m * mstride + a.JH + i] = make_double2(gn.x - gs.x, gn.y - gs.y);
+      }
     }
     __syncthreads();  // the buffer is refilled by the prefetch of the next iteration
   }
@@ -288,19 +300,21 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
   double2 *stw = smem_all, *stwI = smem_all + NC, *sm = smem_all + 2 * NC;
   load_twiddles<T, NC, NT>(a, stw, stwI);
 
+  constexpr int JTh = JT / 2;  // mirrored row pairs per tile
   const int tid = threadIdx.x, r = tid / T, u = tid % T;
-  const int ntile = (a.J + JT - 1) / JT;
+  const int ntile = (a.JH + JTh - 1) / JTh;
   const long long ntot = (long long)a.ncol * ntile;
   const long long mstride = (long long)a.ncolF * a.J;
 
+  // rows [0, JTh) of a staged tile take E (then north), rows [JTh, JT) take O (then south)
   auto issue = [&](long long t, double2 *buf) {
-    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT;
-    const double2 *Fb = a.Fc + (long long)(a.colF0 + col) * a.J + j0;
-    const int nrows = min(JT, a.J - j0);
+    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
+    const double2 *Fb = a.Fc + (long long)(a.colF0 + col) * a.J + h0;
+    const int nh = min(JTh, a.JH - h0);
     for (int idx = tid; idx < (a.N + 1) * JT; idx += NT) {
-      const int m = idx / JT, rr = idx - m * JT;
-      const bool in = rr < nrows;
-      cp_async16(buf + m * JTp + rr, in ? Fb + m * mstride + rr : Fb, in);
+      const int m = idx / JT, rr = idx - m * JT, i = rr % JTh;
+      const bool in = i < nh;
+      cp_async16(buf + m * JTp + rr, in ? Fb + m * mstride + (rr < JTh ? 0 : a.JH) + i : Fb, in);
     }
   };
 
@@ -314,8 +328,17 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
     cp_async_wait<1>();
     __syncthreads();
 
-    const int col = (int)(t / ntile), j0 = (int)(t - (long long)col * ntile) * JT, j = j0 + r;
-    const bool valid = j < a.J;
+    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
+    const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
+    const bool valid = jh < a.JH;
+
+    // this row's G^m: north = E + O (rows < JTh), south = E - O
+    const int ri = r % JTh;
+    const double sgn = r < JTh ? 1.0 : -1.0;
+    auto gm = [&](int k) {
+      const double2 e = cur[k * JTp + ri], o = cur[k * JTp + JTh + ri];
+      return make_double2(e.x + sgn * o.x, e.y + sgn * o.y);
+    };
 
     // real pack: Z_k = (X_k + Y_k) + i w^k (X_k - Y_k), Y_k = conj X_{NC-k}, w = e^{+2 pi i/I}
     double2 v[R1];
@@ -324,12 +347,12 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
       const int k = R2 * n1 + u;
       double2 X = make_double2(0.0, 0.0), Y = make_double2(0.0, 0.0);
       if (k <= a.N) {
-        X = cur[k * JTp + r];
+        X = gm(k);
         if (k == 0) X.y = 0.0;
       }
       const int kk = NC - k;
       if (k > 0 && kk <= a.N) {
-        const double2 q = cur[kk * JTp + r];
+        const double2 q = gm(kk);
         Y = make_double2(q.x, -q.y);
       }
       const double2 wI = stwI[k];
@@ -382,21 +405,29 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
 // G^0_j = s_j q_j (forward) and q_j = s_j Re G^0_j (inverse).
 __global__ void __launch_bounds__(256) k_zonal_fwd(FftArgs a)
 {
-  const long long total = (long long)a.ncol * a.J;
+  const long long total = (long long)a.ncol * a.JH;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
-    const int col = (int)(k / a.J), j = (int)(k - (long long)col * a.J);
+    const int col = (int)(k / a.JH), jh = (int)(k - (long long)col * a.JH);
+    const int jn = a.JH + jh, js = a.JH - 1 - jh;
     const double *src = a.gcol ? a.gcol[col] : (col < a.nsplit) ? a.g0 + (long long)col * a.J : a.g1 + (long long)(col - a.nsplit) * a.J;
-    a.F[(long long)(a.colF0 + col) * a.J + j] = make_double2(src[j] * __ldg(a.rowscale + j), 0.0);
+    const double gn = src[jn] * __ldg(a.rowscale + jn), gs = src[js] * __ldg(a.rowscale + js);
+    double2 *F = a.F + (long long)(a.colF0 + col) * a.J;
+    F[jh] = make_double2(gn + gs, 0.0);
+    F[a.JH + jh] = make_double2(gn - gs, 0.0);
   }
 }
 
 __global__ void __launch_bounds__(256) k_zonal_inv(FftArgs a)
 {
-  const long long total = (long long)a.ncol * a.J;
+  const long long total = (long long)a.ncol * a.JH;
   for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < total; k += (long long)gridDim.x * blockDim.x) {
-    const int col = (int)(k / a.J), j = (int)(k - (long long)col * a.J);
+    const int col = (int)(k / a.JH), jh = (int)(k - (long long)col * a.JH);
+    const int jn = a.JH + jh, js = a.JH - 1 - jh;
     double *dst = a.ocol ? a.ocol[col] : (col < a.nsplit) ? a.o0 + (long long)col * a.J : a.o1 + (long long)(col - a.nsplit) * a.J;
-    dst[j] = a.Fc[(long long)(a.colF0 + col) * a.J + j].x * __ldg(a.rowscale + j);
+    const double2 *F = a.Fc + (long long)(a.colF0 + col) * a.J;
+    const double e = F[jh].x, o = F[a.JH + jh].x;
+    dst[jn] = (e + o) * __ldg(a.rowscale + jn);
+    dst[js] = (e - o) * __ldg(a.rowscale + js);
   }
 }
 
@@ -433,7 +464,7 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s
   using S = FftShape<A, B, kFftThreads>;
   const int bufe = S::buf_elems(p->N);
   const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)bufe);
-  const long long ntiles = (long long)args.ncol * ((p->J + S::JT - 1) / S::JT);
+  const long long ntiles = (long long)args.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
   if (ntiles <= 0) return SHT_OK;
   if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
   cudaError_t e = cudaSuccess;
@@ -453,7 +484,7 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s
 int dispatch(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s)
 {
   if (p->zonal) {
-    const long long total = (long long)args.ncol * p->J;
+    const long long total = (long long)args.ncol * p->JH;
     if (total <= 0) return SHT_OK;
     long long g = (total + 255) / 256;
     if (g > 148 * 8) g = 148 * 8;
@@ -486,7 +517,7 @@ int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int ns
   a.F = F; a.ncolF = ncolF; a.colF0 = colF0;
   a.rowscale = p->d_rowscale + (size_t)rs * p->J;
   a.tw = p->d_tw; a.twI = p->d_twI;
-  a.I = p->I; a.J = p->J; a.N = p->N;
+  a.I = p->I; a.J = p->J; a.JH = p->JH; a.N = p->N;
   return dispatch(false, p, a, s);
 }
 
@@ -499,7 +530,7 @@ int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, in
   a.Fc = F; a.ncolF = ncolF; a.colF0 = colF0;
   a.rowscale = p->d_rowscale + (size_t)rs * p->J;
   a.tw = p->d_tw; a.twI = p->d_twI;
-  a.I = p->I; a.J = p->J; a.N = p->N;
+  a.I = p->I; a.J = p->J; a.JH = p->JH; a.N = p->N;
   return dispatch(true, p, a, s);
 }
 

@@ -3,11 +3,13 @@
 // Analysis (space_discretization.tex:197-200), per m and 16 complex
 // field-level columns:
 //     c_n = sum_{jh} Pbar_n^m(mu_jh) * (n-m even ? Gs : Ga)[jh],
-//     Gs/Ga = G(mu_N) +- G(mu_S) over the mirrored Gauss rows (the Gauss
-//     weight is already folded into G by the longitude transform).
+//     Gs/Ga = G(mu_N) +- G(mu_S) over the mirrored Gauss rows, which the
+//     longitude transform delivers at F[m][col][jh] and F[m][col][JH + jh]
+//     (the Gauss weight already folded in).
 // Synthesis (:212-216):
-//     Ge/Go[jh] = sum_{n-m even/odd} Pbar_n^m(mu_jh) a_n,
-//     G(mu_N) = Ge + Go, G(mu_S) = Ge - Go.
+//     Ge/Go[jh] = sum_{n-m even/odd} Pbar_n^m(mu_jh) a_n, written to
+//     F[m][col][jh] and F[m][col][JH + jh]; the inverse longitude transform
+//     forms G(mu_N) = Ge + Go and G(mu_S) = Ge - Go.
 // Both are dense contractions run on the FP64 tensor pipe with
 // mma.sync.m8n8k4.f64 (16 rows x 32 real columns per warp).  A thread block
 // owns one m and one 16-column tile.  Its 8 warps split the rows (analysis) or
@@ -82,19 +84,19 @@ __global__ void __launch_bounds__(kThreads) k_leg_fwd_dmma(LegArgs a)
 
   for (int k0 = 0; k0 < JH; k0 += kKC) {
     const int kc = min(kKC, JH - k0);
-    // stage Gs/Ga for this chunk: 16 columns x 32 latitudes
+    // stage Gs/Ga for this chunk: 16 columns x 32 half-latitudes
     for (int idx = tid; idx < kCT * kKC; idx += kThreads) {
       const int jh = idx % kKC, c = idx / kKC;
-      double2 fn = make_double2(0.0, 0.0), fs = fn;
+      double2 gs = make_double2(0.0, 0.0), ga = gs;
       if (jh < kc && col0 + c < a.ncol) {
         const double2 *Fc = a.F + ((long long)m * a.ncol + col0 + c) * a.J;
-        fn = Fc[JH + k0 + jh];
-        fs = Fc[JH - 1 - k0 - jh];
+        gs = Fc[k0 + jh];
+        ga = Fc[JH + k0 + jh];
       }
-      Gs[jh][2 * c] = fn.x + fs.x;
-      Gs[jh][2 * c + 1] = fn.y + fs.y;
-      Ga[jh][2 * c] = fn.x - fs.x;
-      Ga[jh][2 * c + 1] = fn.y - fs.y;
+      Gs[jh][2 * c] = gs.x;
+      Gs[jh][2 * c + 1] = gs.y;
+      Ga[jh][2 * c] = ga.x;
+      Ga[jh][2 * c + 1] = ga.y;
     }
     __syncthreads();
 #pragma unroll
@@ -283,7 +285,7 @@ __global__ void __launch_bounds__(kThreads) k_leg_inv_dmma(LegArgs a)
       }
     }
   }
-  // G(mu_N) = Ge + Go at j = JH + jh, G(mu_S) = Ge - Go at j = JH - 1 - jh
+  // Ge at F[m][col][jh], Go at F[m][col][JH + jh]
 #pragma unroll
   for (int q = 0; q < MAXU; ++q) {
     const int u = warp + kWarps * q;
@@ -300,8 +302,8 @@ __global__ void __launch_bounds__(kThreads) k_leg_inv_dmma(LegArgs a)
         const double er = acc[q][0][t][nt][0], ei = acc[q][0][t][nt][1];
         const double orr = acc[q][1][t][nt][0], oi = acc[q][1][t][nt][1];
         double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * a.J;
-        Fc[JH + jh] = make_double2(er + orr, ei + oi);
-        Fc[JH - 1 - jh] = make_double2(er - orr, ei - oi);
+        Fc[jh] = make_double2(er, ei);
+        Fc[JH + jh] = make_double2(orr, oi);
       }
     }
   }

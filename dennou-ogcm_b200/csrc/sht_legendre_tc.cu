@@ -290,23 +290,24 @@ __device__ void column_exponents(const TcArgs &a, const Sub &s, int col0, const 
   double m0 = 0.0, m1 = 0.0;
   // loads are issued 8 at a time so that they are in flight together
   if (!INV) {
-    // both parities of band m over all latitudes (done at the first chunk of (m, 0))
+    // Gs (parity 0) at jh and Ga (parity 1) at JH + jh, over all half-latitudes
+    // (done at the first chunk of (m, 0))
     const double *col = reinterpret_cast<const double *>(a.F + ((long long)s.m * a.ncol + (valid ? b : 0)) * a.J) + part;
     const int JH = a.JH, hh = (JH + 1) / 2;
     const int j0 = half * hh, j1 = min(JH, (half + 1) * hh);
     if (valid)
       for (int jb = j0; jb < j1; jb += 8) {
-        double gn[8], gs[8];
+        double gs[8], ga[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
           const int jh = min(jb + q, j1 - 1);
-          gn[q] = col[2 * (JH + jh)];
-          gs[q] = col[2 * (JH - 1 - jh)];
+          gs[q] = col[2 * jh];
+          ga[q] = col[2 * (JH + jh)];
         }
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-          m0 = fmax(m0, fabs(gn[q] + gs[q]));
-          m1 = fmax(m1, fabs(gn[q] - gs[q]));
+          m0 = fmax(m0, fabs(gs[q]));
+          m1 = fmax(m1, fabs(ga[q]));
         }
       }
   } else {
@@ -350,20 +351,21 @@ __device__ void prepare(const TcArgs &a, const Sub &s, int h, int col0, const Sm
     uint4 pk[kS];
     unsigned short *pkh = reinterpret_cast<unsigned short *>(pk);
     if (!INV) {
-      const double *col = reinterpret_cast<const double *>(a.F + ((long long)s.m * a.ncol + (valid ? b : 0)) * a.J) + part;
+      // Gs (p = 0) at jh, Ga (p = 1) at JH + jh
+      const double *col = reinterpret_cast<const double *>(a.F + ((long long)s.m * a.ncol + (valid ? b : 0)) * a.J) +
+                          part + 2 * s.p * JH;
       const double sc = ldexp(1.0, -e);
-      double gn[8], gs[8];
+      double gv[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int jh = min(h * kKC + kg * 8 + q, JH - 1);
-        gn[q] = valid ? col[2 * (JH + jh)] : 0.0;
-        gs[q] = valid ? col[2 * (JH - 1 - jh)] : 0.0;
+        gv[q] = valid ? col[2 * jh] : 0.0;
       }
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
         const int jh = h * kKC + kg * 8 + q;
         double x = 0.0;
-        if (jh < JH) x = (s.p ? gn[q] - gs[q] : gn[q] + gs[q]) * sc;
+        if (jh < JH) x = gv[q] * sc;
         unsigned short d[kS];
         digits_bf16(x, d);
 #pragma unroll
@@ -443,28 +445,14 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
           reinterpret_cast<double *>(a.S + (rowbase + s.p + 2 * n) * a.ncol + b)[part] = ldexp(acc[i], e + fe[n] - 14);
       }
     } else {
-      // The even half is parked in this thread's northern output slots and
-      // combined with the odd half on the second pass (same thread, same addresses).
+      // even-degree sums at F[m][col][jh], odd at F[m][col][JH + jh]
       const int *ge = a.texp + (s.m * 2 + s.p) * a.JH;
-      double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + b) * a.J) + part;
-      const int JH = a.JH;
-      double gev[16];
+      double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + b) * a.J) + part + 2 * s.p * a.JH;
       const int j0 = s.row0 + 16 * g;
-      if (s.p == 1) {
-#pragma unroll
-        for (int i = 0; i < 16; ++i) gev[i] = (j0 + i < JH) ? Fc[2 * (JH + j0 + i)] : 0.0;
-      }
 #pragma unroll
       for (int i = 0; i < 16; ++i) {
         const int jh = j0 + i;
-        if (jh >= JH) continue;
-        const double v = ldexp(acc[i], e + ge[jh] - 14);
-        if (s.p == 0) {
-          Fc[2 * (JH + jh)] = v;
-        } else {
-          Fc[2 * (JH + jh)] = gev[i] + v;
-          Fc[2 * (JH - 1 - jh)] = gev[i] - v;
-        }
+        if (jh < a.JH) Fc[2 * jh] = ldexp(acc[i], e + ge[jh] - 14);
       }
     }
   }

@@ -16,7 +16,9 @@
 // smaller); larger grids use the chunked kernels of sht_legendre.cu.
 //
 // Analysis follows space_discretization.tex:197-200 and synthesis :212-216.
-// Symmetric and antisymmetric latitude halves use Pbar(-mu) = (-1)^{n-m} Pbar(mu).
+// Symmetric and antisymmetric latitude halves use Pbar(-mu) = (-1)^{n-m} Pbar(mu);
+// the longitude transforms deliver Gs/Ga and take the even/odd-degree sums at
+// F[m][col][jh] and F[m][col][JH + jh].
 #include "sht_internal.h"
 #include "sht_dmma.cuh"
 
@@ -105,25 +107,6 @@ __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma
   }
 }
 
-// In place: row [j] of a column -> Gs at jh, Ga at JH + jh (jh = 0..JH-1)
-template <int JH>
-__device__ void combine_panels(const Geo &g, double *buf, int nm)
-{
-  constexpr int half = JH / 2;
-  const int total = nm * kCT * half;
-  for (int q = threadIdx.x; q < total; q += kT) {
-    const int row = q / half, jh = q % half;
-    double2 *G = reinterpret_cast<double2 *>(buf + row * g.CS);
-    const int jq = JH - 1 - jh;
-    const double2 s0 = G[jh], s1 = G[jq];            // south rows JH-1-jq, JH-1-jh
-    const double2 n0 = G[JH + jh], n1 = G[JH + jq];  // north rows
-    G[jh] = make_double2(n0.x + s1.x, n0.y + s1.y);        // Gs(jh)  = G(JH+jh) + G(JH-1-jh)
-    G[jq] = make_double2(n1.x + s0.x, n1.y + s0.y);        // Gs(jq)
-    G[JH + jh] = make_double2(n0.x - s1.x, n0.y - s1.y);   // Ga(jh)
-    G[JH + jq] = make_double2(n1.x - s0.x, n1.y - s0.y);   // Ga(jq)
-  }
-}
-
 template <int JH>
 __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
 {
@@ -158,10 +141,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
     cp_commit();
     cp_wait1();
     __syncthreads();
-    const int nm = (pr.y >= 0) ? 2 : 1;
-    double *const Gcur = bsel ? G1 : G0;
-    combine_panels<JH>(g, Gcur, nm);
-    __syncthreads();
+    double *const Gcur = bsel ? G1 : G0;  // column rows: Gs at [0, JH), Ga at [JH, J)
 
     // jobs: (band, parity, 16-row group)
     const int Ra = a.N + 2 - pr.x, Rb = (pr.y >= 0) ? a.N + 2 - pr.y : 0;
@@ -307,9 +287,8 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
         const int c = col0 + 4 * (grp * nnt + q) + (lane & 3);
         if (c >= a.ncol) continue;
         double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
-        const double er = acc[0][q][0], ei = acc[0][q][1], orr = acc[1][q][0], oi = acc[1][q][1];
-        Fc[JH + jh] = make_double2(er + orr, ei + oi);
-        Fc[JH - 1 - jh] = make_double2(er - orr, ei - oi);
+        Fc[jh] = make_double2(acc[0][q][0], acc[0][q][1]);       // even degrees
+        Fc[JH + jh] = make_double2(acc[1][q][0], acc[1][q][1]);  // odd degrees
       }
     }
     __syncthreads();

@@ -13,18 +13,18 @@
 // bound the fill.
 //
 //   analysis:  chunk = KC half-latitudes jh: the P rows of both bands for those
-//              jh, and per column the north run JH+jh and the mirrored south
-//              run, folded in place into Gs/Ga.  Each warp keeps up to JPW
+//              jh, and per column the runs of Gs and Ga (delivered by the
+//              longitude transform at jh and JH + jh).  Each warp keeps up to JPW
 //              (16 degrees x 32 real columns) accumulator blocks in registers
 //              over the chunks of an item.
 //   synthesis: chunk = KL half-latitudes of the output (32, or 16 at T341);
 //              the coefficient panel of the item (both bands, all degrees) is
 //              resident.  Each warp owns one 8-latitude tile for one parity and
 //              4 (KL = 32) or 2 (KL = 16) of the four 8-column tiles, so each P
-//              fragment feeds that many products; the two parities meet through
-//              shared memory to form the north and south rows.  Rows past a
-//              band's last degree are zero coefficients (and finite P rows), so
-//              the degree loop needs no bounds checks.
+//              fragment feeds that many products, and writes its parity's sums
+//              (the inverse longitude transform forms the north and south rows).
+//              Rows past a band's last degree are zero coefficients (and finite
+//              P rows), so the degree loop needs no bounds checks.
 //
 // The symmetric/antisymmetric split is Pbar(-mu) = (-1)^{n-m} Pbar(mu); the
 // analysis follows space_discretization.tex:197-200, the synthesis :212-216.
@@ -83,35 +83,16 @@ __device__ void issue_fwd_chunk(const V3Args &a, double *Pst, double *Gst, int2 
     const double *src = (row < Ra ? Pa + (long long)row * a.JH : Pb + (long long)(row - Ra) * a.JH) + 2 * ch;
     cp16(Pst + row * G::PS + 2 * ch, src, true);
   }
-  // per column row: north latitudes JH+k0.. and the mirrored south run JH-k0-KC..
+  // per column row: the Gs run at jh = k0.. and the Ga run at JH + k0..
   const int nrow = (pr.y >= 0 ? 2 : 1) * kCT;
   for (int q = threadIdx.x; q < nrow * 2 * KC; q += kT) {
     const int row = q / (2 * KC), e = q % (2 * KC);
     const int run = e / KC, i = e % KC;
     const int b = row % kCT, m = (row < kCT) ? pr.x : pr.y;
     const bool ok = col0 + b < a.ncol;
-    const int j = run == 0 ? a.JH + k0 + i : a.JH - k0 - KC + i;
+    const int j = run * a.JH + k0 + i;
     const double2 *src = ok ? a.F + ((long long)m * a.ncol + col0 + b) * a.J + j : a.F;
     cp16(Gst + row * G::CS + 2 * (run * KC + i), src, ok);
-  }
-}
-
-// In place: north run n[i] and south run s[i] (s[KC-1-i] mirrors n[i]) ->
-// Gs[i] = n[i] + s[KC-1-i] over the north run, Ga[i] = n[i] - s[KC-1-i]
-// over the south run.
-template <int KC>
-__device__ void combine_chunk(double *Gst, int nrow)
-{
-  using G = FwdGeo<KC>;
-  constexpr int H = KC / 2;
-  for (int q = threadIdx.x; q < nrow * H; q += kT) {
-    const int row = q / H, i = q % H, k = KC - 1 - i;
-    double2 *g = reinterpret_cast<double2 *>(Gst + row * G::CS);
-    const double2 ni = g[i], nk = g[k], si = g[KC + i], sk = g[KC + k];
-    g[i] = make_double2(ni.x + sk.x, ni.y + sk.y);
-    g[k] = make_double2(nk.x + si.x, nk.y + si.y);
-    g[KC + i] = make_double2(ni.x - sk.x, ni.y - sk.y);
-    g[KC + k] = make_double2(nk.x - si.x, nk.y - si.y);
   }
 }
 
@@ -164,8 +145,6 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_chunk(V3Args a)
       issue_fwd_chunk<KC>(a, st ? P0 : P1, st ? G0 : G1, a.pairs[itn / a.ntiles], (itn % a.ntiles) * kCT, kn * KC);
     }
     cp_commit();
-    combine_chunk<KC>(Gc, (pr.y >= 0 ? 2 : 1) * kCT);
-    __syncthreads();
 
     const Jobs jb(a.N, pr);
     if (kc == 0) {
@@ -352,17 +331,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_chunk(V3Args a)
         pb += 8 * kAS;
       }
     }
-    // the parities meet in the P stage just used (free after this barrier)
-    __syncthreads();
-    double2 *X = reinterpret_cast<double2 *>(Pc);  // [warp][band][tile][lane]
-#pragma unroll
-    for (int mi = 0; mi < 2; ++mi)
-#pragma unroll
-      for (int ct = 0; ct < CPW; ++ct)
-        X[((warp * 2 + mi) * CPW + ct) * 32 + lane] = make_double2(acc[mi][ct][0], acc[mi][ct][1]);
-    __syncthreads();
-    // parity-0 warps write the north rows (even + odd), parity-1 warps the south rows (even - odd)
-    const int other = warp ^ NLT;
+    // each warp writes its parity: even-degree sums at F[m][col][jh], odd at JH + jh
     const int jh = kc * KL + 8 * lt + (lane >> 2);
 #pragma unroll
     for (int mi = 0; mi < 2; ++mi) {
@@ -371,11 +340,8 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_chunk(V3Args a)
 #pragma unroll
       for (int ct = 0; ct < CPW; ++ct) {
         const int col = col0 + 4 * (CPW * cg + ct) + (lane & 3);
-        const double2 q = X[((other * 2 + mi) * CPW + ct) * 32 + lane];  // the partner parity
         if (col >= a.ncol) continue;
-        double2 *Fc = a.Fo + ((long long)m * a.ncol + col) * a.J;
-        if (par == 0) Fc[a.JH + jh] = make_double2(acc[mi][ct][0] + q.x, acc[mi][ct][1] + q.y);
-        else Fc[a.JH - 1 - jh] = make_double2(q.x - acc[mi][ct][0], q.y - acc[mi][ct][1]);
+        a.Fo[((long long)m * a.ncol + col) * a.J + par * a.JH + jh] = make_double2(acc[mi][ct][0], acc[mi][ct][1]);
       }
     }
   }
@@ -417,9 +383,7 @@ bool choose(const sht_plan *p, Choice *c)
   const size_t ast = (size_t)coef_rows(p->N) * kAS;
   c->DB = sizeof(double) * (2 * pst + 2 * ast) <= lim;
   c->inv_smem = sizeof(double) * (2 * pst + (c->DB ? 2 : 1) * ast);
-  // the parity exchange (8 warps x 2 bands x 4 tiles' worth of lanes, double2) fits in one P stage
-  const bool xfits = pst >= (size_t)kW * 2 * 4 * 32 * 2;
-  return xfits && c->fwd_smem <= lim && c->inv_smem <= lim;
+  return c->fwd_smem <= lim && c->inv_smem <= lim;
 }
 
 template <typename K>
