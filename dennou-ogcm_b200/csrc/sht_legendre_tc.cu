@@ -52,7 +52,9 @@ namespace {
 
 constexpr int kS = 7;                      // digits per operand
 constexpr int kAcc = 5;                    // TMEM accumulators: levels 0, 1, 2, 3 and 4..6
-constexpr int kSeg = 96;                   // output columns per segment (kAcc x kSeg <= 512 TMEM columns)
+constexpr int kSeg = 96;                   // analysis: output columns per segment (kAcc x kSeg <= 512 TMEM columns)
+constexpr int kSegInv = 64;                // synthesis with output staging: Gauss rows per segment
+constexpr int kStg = 2 * 16 + 2;           // doubles per field-level row of the synthesis output staging
 constexpr int kKC = 32;                    // K per chunk (2 MMA K-steps of 16)
 constexpr int kM = 128;                    // data columns per CTA (64 complex)
 constexpr int kRowB = kKC * 2;             // 64 bytes per row of one digit tile
@@ -191,6 +193,7 @@ struct TcArgs {
   int ntiles, nitems, per_cta;
   int npad_max;       // TMEM columns per accumulator (largest segment)
   int npad_max_table; // rows of one synthesis digit tile (latitudes, padded)
+  int seg_inv;        // synthesis segment (kSegInv with staged output, else kSeg)
   int *err;
 };
 
@@ -208,10 +211,11 @@ __device__ __forceinline__ Sub make_sub(const TcArgs &a, int m, int p, int seg, 
   s.p = p;
   s.Rp = rows_of_parity(a.N, m, p);
   s.nrow = INV ? a.JH : s.Rp;  // output rows of the sub-item
-  s.nseg = (s.nrow + kSeg - 1) / kSeg;
+  const int cap = INV ? a.seg_inv : kSeg;
+  s.nseg = (s.nrow + cap - 1) / cap;
   s.seg = seg;
-  s.row0 = seg * kSeg;
-  s.npad = round_up(min(kSeg, s.nrow - s.row0), 16);
+  s.row0 = seg * cap;
+  s.npad = round_up(min(cap, s.nrow - s.row0), 16);
   s.nch = INV ? (s.Rp + kKC - 1) / kKC : (a.JH + kKC - 1) / kKC;
   s.slot = q & 3;
   return s;
@@ -278,6 +282,7 @@ struct Smem {
   unsigned char *B[2];
   int *exps;      // [4 slots][128 columns]
   double *part;   // [2][2][128] partial maxima
+  double *stage;  // synthesis: [2 halves][64 field-levels][kStg] output staging
 };
 
 // Column exponents of the sub-items that start at this chunk.
@@ -423,19 +428,21 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
   const uint32_t lane_base = tbase + ((uint32_t)((warp & 3) * 32) << 16);
   const int ngroups = s.npad / 16;
   for (int g = half; g < ngroups; g += 2) {
+    // all accumulators of the group in flight at once, one wait
+    uint32_t r[kAcc][16];
+#pragma unroll
+    for (int d = 0; d < kAcc; ++d) tc::tmem_ld16(lane_base + (uint32_t)(d * a.npad_max + 16 * g), r[d]);
+    tc::tmem_wait_ld();
     double acc[16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) acc[i] = 0.0;
+    for (int i = 0; i < 16; ++i) {
+      double t = 0.0;
 #pragma unroll
-    for (int d = kAcc - 1; d >= 0; --d) {  // smallest first
-      uint32_t r[16];
-      tc::tmem_ld16(lane_base + (uint32_t)(d * a.npad_max + 16 * g), r);
-      tc::tmem_wait_ld();
-#pragma unroll
-      for (int i = 0; i < 16; ++i) acc[i] += (double)__uint_as_float(r[i]);
+      for (int d = kAcc - 1; d >= 0; --d) t += (double)__uint_as_float(r[d][i]);  // smallest first
+      acc[i] = t;
     }
-    if (!valid) continue;
     if (!INV) {
+      if (!valid) continue;
       const int *fe = a.texp + a.teoff[s.m * 2 + s.p];
       const long long rowbase = a.rowoff[s.m];
 #pragma unroll
@@ -444,8 +451,10 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
         if (n < s.Rp)
           reinterpret_cast<double *>(a.S + (rowbase + s.p + 2 * n) * a.ncol + b)[part] = ldexp(acc[i], e + fe[n] - 14);
       }
-    } else {
-      // even-degree sums at F[m][col][jh], odd at F[m][col][JH + jh]
+    } else if (a.seg_inv != kSegInv) {
+      // even-degree sums at F[m][col][jh], odd at F[m][col][JH + jh], straight
+      // from the registers (no room for the staging next to 96-row segments)
+      if (!valid) continue;
       const int *ge = a.texp + (s.m * 2 + s.p) * a.JH;
       double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + b) * a.J) + part + 2 * s.p * a.JH;
       const int j0 = s.row0 + 16 * g;
@@ -454,6 +463,30 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
         const int jh = j0 + i;
         if (jh < a.JH) Fc[2 * jh] = ldexp(acc[i], e + ge[jh] - 14);
       }
+    } else {
+      // staged per half of the CTA so that each warp writes 256-byte runs of
+      // one field-level
+      const int *ge = a.texp + (s.m * 2 + s.p) * a.JH;
+      const int j0 = s.row0 + 16 * g;
+      double *stg = sm.stage + half * 64 * kStg;
+#pragma unroll
+      for (int i = 0; i < 16; ++i) {
+        const int jh = j0 + i;
+        stg[(c >> 1) * kStg + 2 * i + part] = (jh < a.JH) ? ldexp(acc[i], e + ge[jh] - 14) : 0.0;
+      }
+      asm volatile("bar.sync %0, 128;\n" ::"r"(1 + half));
+      const int wl = warp & 3, lane = tid & 31;
+      const int i = lane >> 1, prt = lane & 1;
+      if (j0 + i < a.JH) {
+#pragma unroll 4
+        for (int q = 0; q < 16; ++q) {
+          const int bl = 16 * wl + q, col = col0 + bl;
+          if (col < a.ncol)
+            reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + col) * a.J + s.p * a.JH + j0 + i)[prt] =
+                stg[bl * kStg + lane];
+        }
+      }
+      asm volatile("bar.sync %0, 128;\n" ::"r"(1 + half));
     }
   }
 }
@@ -472,6 +505,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_split(TcArgs a)
   sm.B[1] = sm.B[0] + bstage;
   sm.exps = reinterpret_cast<int *>(sm.B[1] + bstage);
   sm.part = reinterpret_cast<double *>(sm.exps + 4 * 128);
+  sm.stage = sm.part + 4 * 128;
   const int tid = threadIdx.x, warp = tid >> 5;
 
   const int it0 = blockIdx.x * a.per_cta;
@@ -620,9 +654,10 @@ int build_split_tables(sht_plan *p)
   return SHT_OK;
 }
 
-size_t split_smem(int npad_max)
+size_t split_smem(int npad_max, bool staged)
 {
-  return 2 * (size_t)kS * kM * kRowB + 2 * (size_t)kS * npad_max * kRowB + 4 * 128 * sizeof(int) + 4 * 128 * sizeof(double);
+  return 2 * (size_t)kS * kM * kRowB + 2 * (size_t)kS * npad_max * kRowB + 4 * 128 * sizeof(int) + 4 * 128 * sizeof(double) +
+         (staged ? 2 * 64 * (size_t)kStg * sizeof(double) : 0);
 }
 
 int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2 *out, cudaStream_t s)
@@ -639,7 +674,9 @@ int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2
   TcArgs a{};
   if (inverse) {
     a.Sc = in; a.Fo = out; a.tab = t->inv; a.toff = t->inv_off; a.texp = t->inv_exp;
-    a.npad_max = t->inv_npad < kSeg ? t->inv_npad : kSeg;
+    // staged output (64-row segments) where its buffer fits beside the stages
+    a.seg_inv = split_smem(kSegInv, true) <= 227 * 1024 && p->JH <= 128 ? kSegInv : kSeg;
+    a.npad_max = t->inv_npad < a.seg_inv ? t->inv_npad : a.seg_inv;
     a.npad_max_table = t->inv_npad;
   } else {
     a.F = in; a.S = out; a.tab = t->fwd; a.toff = t->fwd_off; a.texp = t->fwd_exp; a.teoff = t->fwd_eoff;
@@ -652,7 +689,7 @@ int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2
   const int slots = p->num_sms;
   a.per_cta = (a.nitems + slots - 1) / slots;
   const int grid = (a.nitems + a.per_cta - 1) / a.per_cta;
-  const size_t smem = split_smem(a.npad_max);
+  const size_t smem = split_smem(a.npad_max, inverse && a.seg_inv == kSegInv);
   auto kern = inverse ? k_leg_split<true> : k_leg_split<false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return cuda_fail(e, "split smem attribute");
@@ -671,7 +708,7 @@ bool split_supported(const sht_plan *p)
   // degrees of one parity (synthesis).
   static_assert(kAcc * kSeg <= 512, "TMEM columns");
   const int Rmax = (p->N + 3) / 2;
-  return p->JH <= 256 && Rmax <= 256 && split_smem(kSeg) <= 227 * 1024;
+  return p->JH <= 256 && Rmax <= 256 && split_smem(kSeg, false) <= 227 * 1024;
 }
 
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
