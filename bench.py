@@ -39,6 +39,15 @@ METRIC = "T85L60 round-trip transforms/s: split-prec TC vs FP64 GPU, ≤1e-11 re
 UNIT = "round-trip transforms/s"
 GRID = "T85"
 LEVELS, FIELDS, POWER = 60, 8, 2.0
+# the configurations' (levels, fields) per grid, for --grid runs at other
+# resolutions (C0 T21 L20 x 3, C1 T85 L60 x 8, C2 T170 L60 x 12, C4 T341 L60 x 16)
+GRID_BATCH = {"T21": (20, 3), "T42": (60, 8), "T85": (60, 8), "T170": (60, 12), "T341": (60, 16)}
+
+
+def _workload(grid):
+    lv, fd = GRID_BATCH[grid]
+    metric = METRIC if grid == GRID else METRIC.replace("T85L60", f"{grid}L{lv}")
+    return lv, fd, metric
 RADIUS = 6.371e6
 
 
@@ -50,11 +59,11 @@ def _peaks():
         return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
 
 
-def _traffic(kernel, mode, nb):
+def _traffic(kernel, mode, nb, grid=GRID):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     capture of this workload (profiles/t85_roundtrip_fp64.md), FP64 path at the
     480 field-level batch; None for any other configuration."""
-    if mode != "fp64" or nb != LEVELS * FIELDS:
+    if mode != "fp64" or nb != LEVELS * FIELDS or grid != GRID:
         return None
     try:
         with open(os.path.join(ROOT, "profiles", "t85_dram_traffic.json")) as f:
@@ -148,8 +157,9 @@ def run_reference(args):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     W = importlib.import_module("dennou-ogcm_b200.workloads")
-    I, J, N = W.GRIDS[GRID]
-    nb = args.nb or LEVELS * FIELDS
+    I, J, N = W.GRIDS[args.grid]
+    lv, fd, metric = _workload(args.grid)
+    nb = args.nb or lv * fd
     cores = os.cpu_count() or 1
     O.set_threads(cores)
     p = O.OraclePlan(I, J, N, RADIUS)
@@ -163,11 +173,11 @@ def run_reference(args):
         t.append(time.perf_counter() - t0)
     tot = sum(t)
     value = nb * args.steps / tot
-    rec = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+    rec = {"impl": "reference", "metric": metric, "value": value, "unit": UNIT, "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic (seeded spectra, seed 20261203)",
-           "config": {"workload": f"{GRID} L{LEVELS} x {FIELDS} fields round trip (xy_w then w_xy)",
+           "config": {"workload": f"{args.grid} L{lv} x {fd} fields round trip (xy_w then w_xy)",
                       "field_levels": nb, "im": I, "jm": J, "nm": N},
            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
                             "sample": f"{args.steps} full steps of {nb} field-levels, OpenMP over field-levels"},
@@ -177,11 +187,11 @@ def run_reference(args):
     return 0
 
 
-def cpu_baseline(nb, seconds=10.0):
+def cpu_baseline(nb, grid=GRID, seconds=10.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     W = importlib.import_module("dennou-ogcm_b200.workloads")
-    I, J, N = W.GRIDS[GRID]
+    I, J, N = W.GRIDS[grid]
     cores = os.cpu_count() or 1
     O.set_threads(cores)
     p = O.OraclePlan(I, J, N, RADIUS)
@@ -263,7 +273,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "split"])
-    ap.add_argument("--nb", type=int, default=0, help="field-levels (default 480)")
+    ap.add_argument("--nb", type=int, default=0, help="field-levels (default: the grid's configuration, 480 at T85)")
+    ap.add_argument("--grid", default=GRID, choices=sorted(GRID_BATCH),
+                    help="resolution (default T85, the headline workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-multi", action="store_true", help="skip the C3 multi-instance measurement")
@@ -281,10 +293,11 @@ def main():
 
     P = importlib.import_module("dennou-ogcm_b200")
     W = importlib.import_module("dennou-ogcm_b200.workloads")
-    I, J, N = W.GRIDS[GRID]
-    nb = args.nb or LEVELS * FIELDS
+    I, J, N = W.GRIDS[args.grid]
+    lv, fd, metric = _workload(args.grid)
+    nb = args.nb or lv * fd
     L = (N + 1) ** 2
-    sht = P.SpmlUtil(I, J, LEVELS, N, None, RADIUS)
+    sht = P.SpmlUtil(I, J, lv, N, None, RADIUS)
     lib = P.load_library()
     stream = torch.cuda.current_stream(dev)
 
@@ -399,7 +412,7 @@ def main():
             peak = float(fp64_dmma.value)
             pk_note = "FP64 mma.sync probe measured in this run"
     roofline = {"kernel": name, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                "frac": achieved / peak if peak else None, "traffic": _traffic(name, head_mode, nb),
+                "frac": achieved / peak if peak else None, "traffic": _traffic(name, head_mode, nb, args.grid),
                 "traffic_unit": "DRAM bytes per launch (mean of the forward and inverse kernel)",
                 "algorithmic_per_launch": work / 2, "peak_source": pk_note,
                 "stage_ms_per_step": {"synthesis[fft,legendre,spectral]": st["syn"],
@@ -438,15 +451,15 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(nb)
+        cpu = cpu_baseline(nb, args.grid)
 
     if rank == 0:
         rec = {
-            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "metric": metric, "value": head["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded spectra (n+1)^-2, seed 20261203)",
-            "config": {"workload": f"{GRID} L{LEVELS} x {FIELDS} fields round trip (xya_wa then wa_xya)",
+            "config": {"workload": f"{args.grid} L{lv} x {fd} fields round trip (xya_wa then wa_xya)",
                        "field_levels_per_gpu": nb, "im": I, "jm": J, "nm": N,
                        "precision": head_mode, "l2": "flushed (256 MiB write) between steps, outside the timed events",
                        "parallelism": f"replicas x{world}"},
