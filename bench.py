@@ -266,6 +266,60 @@ def bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world):
     return out
 
 
+def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
+    """The fused clients against their unfused compositions on the headline
+    plan and batch, FP64, CUDA events on the launching stream, L2 flushed
+    between steps outside the events:
+    - product epilogue: w_AlphaOptrProd_xy(A, B, Q) against A*Q, B*Q (torch)
+      followed by w_AlphaOptr_xy (the tracer flux divergence of the thickness
+      equation, Q = H cos(phi) T);
+    - Redi/GM gradients: xy_HGrad_xy(T) against w_xy then xy_GradLon_w and
+      xy_GradLat_w."""
+    nb = args.nb or 480
+    g = torch.Generator(device=dev).manual_seed(20261203)
+    shape = (nb, sht.jm, sht.im)
+    A, B, T = (torch.randn(shape, generator=g, dtype=torch.float64, device=dev) for _ in range(3))
+    Q = 1.0 + 0.5 * torch.randn(shape, generator=g, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sht.set_precision(P.SHT_PREC_FP64)
+
+    def timeit(fn):
+        for _ in range(max(args.warmup, 3)):
+            flush.zero_()
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        return max_over_ranks(tot) / args.steps
+
+    def prod_unfused():
+        return sht.w_AlphaOptr_xy(A * Q, B * Q)
+
+    def hgrad_unfused():
+        w = sht.w_xy(T)
+        return sht.xy_GradLon_w(w), sht.xy_GradLat_w(w)
+
+    fused_p, ref_p = sht.w_AlphaOptrProd_xy(A, B, Q), prod_unfused()
+    (lon, lat), (rlon, rlat) = sht.xy_HGrad_xy(T), hgrad_unfused()
+    torch.cuda.synchronize()
+    out = {"workload": f"{nb} field-levels on the headline grid, fp64"}
+    for name, fused, unfused, err in (
+            ("alphaoptr_prod", lambda: sht.w_AlphaOptrProd_xy(A, B, Q), prod_unfused,
+             _rel(fused_p.cpu().numpy(), ref_p.cpu().numpy())),
+            ("hgrad_xya", lambda: sht.xy_HGrad_xy(T), hgrad_unfused,
+             max(_rel(lon.cpu().numpy(), rlon.cpu().numpy()), _rel(lat.cpu().numpy(), rlat.cpu().numpy())))):
+        tf, tu = timeit(fused), timeit(unfused)
+        out[name] = {"fused_ms": tf, "unfused_ms": tu, "speedup": tu / tf, "relerr_vs_unfused": err}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -279,6 +333,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-multi", action="store_true", help="skip the C3 multi-instance measurement")
+    ap.add_argument("--no-fused", action="store_true", help="skip the fused-client measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -448,6 +503,7 @@ def main():
                "relerr": _rel(wo.numpy(), wh.numpy())}
 
     multi = None if args.no_multi else bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world)
+    fused = None if args.no_fused else bench_fused(P, torch, dev, sht, args, flush, max_over_ranks)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -474,6 +530,7 @@ def main():
             "clocks": head["clocks"],
             "gpu_launches": head["launches"],
             "multi_instance": multi,
+            "fused_clients": fused,
         }
         print(json.dumps(rec))
     sht.final()

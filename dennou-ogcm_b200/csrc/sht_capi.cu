@@ -137,8 +137,10 @@ void finish_timing(sht_plan *p, bool analysis)
 }
 
 // grid inputs g0 (and g1) -> spectral outputs w0 (and w1)
+// (with `mul`, every input field-level k is first multiplied point by point by
+// the grid mul + k I J)
 int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const double *g1, int nb,
-                 double *w0, double *w1)
+                 double *w0, double *w1, const double *mul = nullptr)
 {
   const int nin = g1 ? 2 : 1, ncol = nin * nb;
   Workspace ws;
@@ -146,7 +148,7 @@ int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const doubl
   if (rc) return rc;
   cudaStream_t s = p->stream;
   mark(p, 0, s);
-  if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s))) return rc;
+  if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s, nullptr, mul, nb))) return rc;
   mark(p, 1, s);
   if ((rc = leg_fwd(p, ws.F, ncol, ws.S, s))) return rc;
   mark(p, 2, s);
@@ -177,7 +179,10 @@ int run_synthesis(sht_plan *p, int unpack_op, int rs, const double *w0, const do
 enum Op : int {
   OP_W_XY, OP_XY_W, OP_DIVLAMBDA, OP_DIVMU, OP_GRADLAMBDA, OP_GRADMU, OP_GRADLON, OP_GRADLAT,
   OP_W_ALPHA, OP_XY_ALPHA, OP_UV2VORDIV, OP_VORDIV2UV, OP_LAPLA, OP_LAPLAINV,
-  OP_AVRLONLAT, OP_INTLONLAT, OP_YA_AVRLON, OP_YA_INTLON
+  OP_AVRLONLAT, OP_INTLONLAT, OP_YA_AVRLON, OP_YA_INTLON,
+  OP_W_ALPHA_PROD,  // w_AlphaOptr_xy(A Q, B Q): third input Q
+  OP_HGRAD,         // xy_GradLon_w and xy_GradLat_w of one spectrum
+  OP_HGRAD_G,       // the same of w_xy(grid)
 };
 
 struct OpShape {
@@ -191,6 +196,9 @@ OpShape shape_of(int op)
   case OP_W_XY: case OP_DIVLAMBDA: case OP_DIVMU: return {1, 1, true, false};
   case OP_XY_W: case OP_GRADLAMBDA: case OP_GRADMU: case OP_GRADLON: case OP_GRADLAT: return {1, 1, false, true};
   case OP_W_ALPHA: return {2, 1, true, false};
+  case OP_W_ALPHA_PROD: return {3, 1, true, false};
+  case OP_HGRAD: return {1, 2, false, true};
+  case OP_HGRAD_G: return {1, 2, true, true};
   case OP_XY_ALPHA: return {2, 1, false, true};
   case OP_UV2VORDIV: return {2, 2, true, false};
   case OP_VORDIV2UV: return {2, 2, false, true};
@@ -200,10 +208,22 @@ OpShape shape_of(int op)
 }
 
 // run an operator on device pointers (plan mutex held by the caller)
-int run_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1)
+int run_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
+            const double *i2 = nullptr)
 {
   if (nb == 0) return SHT_OK;
   switch (op) {
+  case OP_W_ALPHA_PROD: return run_analysis(p, PACK_ALPHA, RS_FWD_INV1MMU2, i0, i1, nb, o0, nullptr, i2);
+  case OP_HGRAD: return run_synthesis(p, UNPACK_HGRAD, RS_INV_INVCOS, i0, nullptr, nb, o0, o1);
+  case OP_HGRAD_G: {
+    // the spectra stay in the workspace temp, sized for both steps up front
+    // so that neither step reallocates under it
+    Workspace ws;
+    int rc = ensure_ws(p, 2 * nb, nb, &ws);
+    if (rc) return rc;
+    if ((rc = run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, i0, nullptr, nb, ws.W, nullptr))) return rc;
+    return run_synthesis(p, UNPACK_HGRAD, RS_INV_INVCOS, ws.W, nullptr, nb, o0, o1);
+  }
   case OP_W_XY: return run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, i0, nullptr, nb, o0, nullptr);
   case OP_DIVLAMBDA: return run_analysis(p, PACK_DIVLAMBDA, RS_FWD_INV1MMU2, i0, nullptr, nb, o0, nullptr);
   case OP_DIVMU: return run_analysis(p, PACK_DIVMU, RS_FWD_INV1MMU2, i0, nullptr, nb, o0, nullptr);
@@ -235,14 +255,15 @@ size_t out_count(const sht_plan *p, int op, int nb)
   }
 }
 
-int check_args(const sht_plan *p, int op, const double *i0, const double *i1, int nb, const double *o0, const double *o1)
+int check_args(const sht_plan *p, int op, const double *i0, const double *i1, int nb, const double *o0, const double *o1,
+               const double *i2 = nullptr)
 {
   int rc = check_plan(p);
   if (rc) return rc;
   const OpShape sh = shape_of(op);
   if (nb < 0) { set_error("nb must be >= 0"); return SHT_ERR_INVALID_ARG; }
   if (nb == 0) return SHT_OK;
-  if (!i0 || (sh.nin == 2 && !i1) || !o0 || (sh.nout == 2 && !o1)) {
+  if (!i0 || (sh.nin >= 2 && !i1) || (sh.nin == 3 && !i2) || !o0 || (sh.nout == 2 && !o1)) {
     set_error("null array argument");
     return SHT_ERR_INVALID_ARG;
   }
@@ -250,33 +271,36 @@ int check_args(const sht_plan *p, int op, const double *i0, const double *i1, in
 }
 
 // Device grid arrays are read and written as 16-byte pairs of doubles.
-int check_dev_alignment(int op, const double *i0, const double *i1, const double *o0, const double *o1)
+int check_dev_alignment(int op, const double *i0, const double *i1, const double *o0, const double *o1,
+                        const double *i2 = nullptr)
 {
   const OpShape sh = shape_of(op);
   auto mis = [](const double *x) { return x && (reinterpret_cast<uintptr_t>(x) & 15u) != 0; };
-  if ((sh.in_grid && (mis(i0) || mis(i1))) || (sh.out_grid && (mis(o0) || mis(o1)))) {
+  if ((sh.in_grid && (mis(i0) || mis(i1) || mis(i2))) || (sh.out_grid && (mis(o0) || mis(o1)))) {
     set_error("device grid arrays must be 16-byte aligned");
     return SHT_ERR_INVALID_ARG;
   }
   return SHT_OK;
 }
 
-int api_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1)
+int api_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
+            const double *i2 = nullptr)
 {
-  int rc = check_args(p, op, i0, i1, nb, o0, o1);
+  int rc = check_args(p, op, i0, i1, nb, o0, o1, i2);
   if (rc || nb == 0) return rc;
-  if ((rc = check_dev_alignment(op, i0, i1, o0, o1))) return rc;
+  if ((rc = check_dev_alignment(op, i0, i1, o0, o1, i2))) return rc;
   std::lock_guard<std::mutex> lk(p->mtx);
   DeviceGuard g(p->device);
   if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
-  rc = run_dev(p, op, i0, i1, nb, o0, o1);
+  rc = run_dev(p, op, i0, i1, nb, o0, o1, i2);
   if (!rc) finish_timing(p, !shape_of(op).out_grid);
   return rc;
 }
 
-int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1)
+int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
+             const double *i2 = nullptr)
 {
-  int rc = check_args(p, op, i0, i1, nb, o0, o1);
+  int rc = check_args(p, op, i0, i1, nb, o0, o1, i2);
   if (rc || nb == 0) return rc;
   std::lock_guard<std::mutex> lk(p->mtx);
   DeviceGuard g(p->device);
@@ -295,7 +319,12 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
     p->io_bytes = need;
   }
   double *d = static_cast<double *>(p->d_io);
-  double *di0 = d, *di1 = d + al(nin_each), *do0 = d + al(nin_each) * sh.nin, *do1 = do0 + al(nout_each);
+  double *di0 = d, *di1 = d + al(nin_each), *di2 = d + 2 * al(nin_each);
+  double *do0 = d + al(nin_each) * sh.nin, *do1 = do0 + al(nout_each);
+  const double *hin[3] = {i0, i1, i2};
+  double *din[3] = {di0, di1, di2};
+  // device input k (or null past the operator's inputs), offset by `off` doubles
+  auto dev_in = [&](int k, size_t off) -> const double * { return k < sh.nin ? din[k] + off : nullptr; };
   cudaStream_t s = p->stream;
   // Large transform batches run as a pipeline of chunks: the upload of chunk
   // c+1 (copy_in), the kernels of chunk c (plan stream) and the download of
@@ -311,11 +340,10 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
       if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e, "chunk events");
   }
   if (nchunk == 1) {
-    if ((e = cudaMemcpyAsync(di0, i0, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_fail(e, "H2D");
-    if (sh.nin == 2 && (e = cudaMemcpyAsync(di1, i1, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_fail(e, "H2D");
-    rc = run_dev(p, op, di0, sh.nin == 2 ? di1 : nullptr, nb, do0, sh.nout == 2 ? do1 : nullptr);
+    for (int k = 0; k < sh.nin; ++k)
+      if ((e = cudaMemcpyAsync(din[k], hin[k], sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+        return cuda_fail(e, "H2D");
+    rc = run_dev(p, op, di0, dev_in(1, 0), nb, do0, sh.nout == 2 ? do1 : nullptr, dev_in(2, 0));
     if (rc) return rc;
     if ((e = cudaMemcpyAsync(o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return cuda_fail(e, "D2H");
@@ -329,15 +357,14 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
     for (int c = 0; c < nchunk; ++c) {
       const int b0 = (int)((long long)nb * c / nchunk), b1 = (int)((long long)nb * (c + 1) / nchunk), n = b1 - b0;
       cudaEvent_t ein = p->chunk_ev[2 * c], eout = p->chunk_ev[2 * c + 1];
-      if ((e = cudaMemcpyAsync(di0 + b0 * pin, i0 + b0 * pin, sizeof(double) * n * pin, cudaMemcpyHostToDevice,
-                               p->copy_in)) != cudaSuccess ||
-          (sh.nin == 2 && (e = cudaMemcpyAsync(di1 + b0 * pin, i1 + b0 * pin, sizeof(double) * n * pin,
-                                                cudaMemcpyHostToDevice, p->copy_in)) != cudaSuccess))
-        return cuda_fail(e, "H2D");
+      for (int k = 0; k < sh.nin; ++k)
+        if ((e = cudaMemcpyAsync(din[k] + b0 * pin, hin[k] + b0 * pin, sizeof(double) * n * pin,
+                                 cudaMemcpyHostToDevice, p->copy_in)) != cudaSuccess)
+          return cuda_fail(e, "H2D");
       if ((e = cudaEventRecord(ein, p->copy_in)) != cudaSuccess || (e = cudaStreamWaitEvent(s, ein, 0)) != cudaSuccess)
         return cuda_fail(e, "chunk event");
-      rc = run_dev(p, op, di0 + b0 * pin, sh.nin == 2 ? di1 + b0 * pin : nullptr, n, do0 + b0 * pout,
-                   sh.nout == 2 ? do1 + b0 * pout : nullptr);
+      rc = run_dev(p, op, di0 + b0 * pin, dev_in(1, b0 * pin), n, do0 + b0 * pout,
+                   sh.nout == 2 ? do1 + b0 * pout : nullptr, dev_in(2, b0 * pin));
       if (rc) return rc;
       if ((e = cudaEventRecord(eout, s)) != cudaSuccess || (e = cudaStreamWaitEvent(p->copy_out, eout, 0)) != cudaSuccess)
         return cuda_fail(e, "chunk event");
@@ -661,6 +688,18 @@ int sht_xya_alphaoptr_wa(sht_plan *p, const double *a, const double *b, int nb, 
 { return api_host(p, OP_XY_ALPHA, a, b, nb, x, nullptr); }
 int sht_xya_alphaoptr_wa_dev(sht_plan *p, const double *a, const double *b, int nb, double *x)
 { return api_dev(p, OP_XY_ALPHA, a, b, nb, x, nullptr); }
+int sht_wa_alphaoptr_prod_xya(sht_plan *p, const double *a, const double *b, const double *q, int nb, double *w)
+{ return api_host(p, OP_W_ALPHA_PROD, a, b, nb, w, nullptr, q); }
+int sht_wa_alphaoptr_prod_xya_dev(sht_plan *p, const double *a, const double *b, const double *q, int nb, double *w)
+{ return api_dev(p, OP_W_ALPHA_PROD, a, b, nb, w, nullptr, q); }
+int sht_xya_hgrad_wa(sht_plan *p, const double *w, int nb, double *lon, double *lat)
+{ return api_host(p, OP_HGRAD, w, nullptr, nb, lon, lat); }
+int sht_xya_hgrad_wa_dev(sht_plan *p, const double *w, int nb, double *lon, double *lat)
+{ return api_dev(p, OP_HGRAD, w, nullptr, nb, lon, lat); }
+int sht_xya_hgrad_xya(sht_plan *p, const double *x, int nb, double *lon, double *lat)
+{ return api_host(p, OP_HGRAD_G, x, nullptr, nb, lon, lat); }
+int sht_xya_hgrad_xya_dev(sht_plan *p, const double *x, int nb, double *lon, double *lat)
+{ return api_dev(p, OP_HGRAD_G, x, nullptr, nb, lon, lat); }
 int sht_uvcoslat2vordiv(sht_plan *p, const double *u, const double *v, int nb, double *vor, double *div)
 { return api_host(p, OP_UV2VORDIV, u, v, nb, vor, div); }
 int sht_uvcoslat2vordiv_dev(sht_plan *p, const double *u, const double *v, int nb, double *vor, double *div)

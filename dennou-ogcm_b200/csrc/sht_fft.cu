@@ -124,6 +124,11 @@ struct FftArgs {
   int I, J, JH, N;
   const double *const *gcol;  // optional per-column grid sources (forward)
   double *const *ocol;        // optional per-column grid destinations (inverse)
+  // forward product mode: column col is multiplied point by point by the
+  // grid field mul + (col mod nmul) I J before the transform
+  const double *mul;
+  int nmul;
+  int mul_staged;  // factor rows staged with the tile (else read in the first pass)
 };
 
 // Shared-memory plan of one thread block: the twiddle tables (2 NC entries),
@@ -201,6 +206,16 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
       const int j = rr < JTh ? a.JH + jh : a.JH - 1 - jh;
       if (jh < a.JH) cp_async16(buf + rr * NCp + c, src + (long long)j * NC + c, true);
     }
+    if (a.mul && a.mul_staged) {  // the factor's rows, in the second half of the buffer
+      const double2 *fsrc = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ);
+#pragma unroll 4
+      for (int q = tid; q < JT * NC; q += NT) {
+        const int rr = q / NC, c = q - rr * NC;
+        const int jh = h0 + (rr % JTh);
+        const int j = rr < JTh ? a.JH + jh : a.JH - 1 - jh;
+        if (jh < a.JH) cp_async16(buf + JT * NCp + rr * NCp + c, fsrc + (long long)j * NC + c, true);
+      }
+    }
   };
 
   long long t = blockIdx.x;
@@ -220,6 +235,14 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
     double2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? cur[r * NCp + R2 * n1 + u] : make_double2(0.0, 0.0);
+    if (a.mul && valid) {
+      const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)j * NC;
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const double2 f = a.mul_staged ? cur[JT * NCp + r * NCp + R2 * n1 + u] : __ldg(frow + R2 * n1 + u);
+        v[n1] = make_double2(v[n1].x * f.x, v[n1].y * f.y);
+      }
+    }
     __syncthreads();  // the staged tile is consumed; the buffer is reused below
     dft_reg<A, false>(v);
     double2 *srow = cur + r * RS;
@@ -410,7 +433,12 @@ __global__ void __launch_bounds__(256) k_zonal_fwd(FftArgs a)
     const int col = (int)(k / a.JH), jh = (int)(k - (long long)col * a.JH);
     const int jn = a.JH + jh, js = a.JH - 1 - jh;
     const double *src = a.gcol ? a.gcol[col] : (col < a.nsplit) ? a.g0 + (long long)col * a.J : a.g1 + (long long)(col - a.nsplit) * a.J;
-    const double gn = src[jn] * __ldg(a.rowscale + jn), gs = src[js] * __ldg(a.rowscale + js);
+    double gn = src[jn] * __ldg(a.rowscale + jn), gs = src[js] * __ldg(a.rowscale + js);
+    if (a.mul) {
+      const double *f = a.mul + (long long)(col % a.nmul) * a.J;
+      gn *= f[jn];
+      gs *= f[js];
+    }
     double2 *F = a.F + (long long)(a.colF0 + col) * a.J;
     F[jh] = make_double2(gn + gs, 0.0);
     F[a.JH + jh] = make_double2(gn - gs, 0.0);
@@ -462,7 +490,14 @@ template <int A, int B>
 int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s)
 {
   using S = FftShape<A, B, kFftThreads>;
-  const int bufe = S::buf_elems(p->N);
+  int bufe = S::buf_elems(p->N);
+  FftArgs a = args;
+  if (!inverse && a.mul) {  // room for the factor's tile beside the data tile, where it fits
+    const int two = (2 * S::JT * S::NCp + 7) & ~7;
+    const int want = bufe > two ? bufe : two;
+    a.mul_staged = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)want) <= 227 * 1024;
+    if (a.mul_staged) bufe = want;
+  }
   const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)bufe);
   const long long ntiles = (long long)args.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
   if (ntiles <= 0) return SHT_OK;
@@ -471,7 +506,7 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s
   auto go = [&](auto kern) {
     if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return;
-    kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(args, bufe);
+    kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(a, bufe);
   };
   if (inverse) go(k_fft_inv<A, B, kFftThreads>);
   else go(k_fft_fwd<A, B, kFftThreads>);
@@ -509,10 +544,13 @@ int dispatch(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t 
 }  // namespace
 
 int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
-                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s, const double *const *gcol)
+                   double2 *F, int ncolF, int colF0, int rs, cudaStream_t s, const double *const *gcol,
+                   const double *mul, int nmul)
 {
   FftArgs a{};
   a.gcol = gcol;
+  a.mul = mul;
+  a.nmul = nmul > 0 ? nmul : 1;
   a.g0 = g0; a.g1 = g1 ? g1 : g0; a.nsplit = nsplit; a.ncol = ncol;
   a.F = F; a.ncolF = ncolF; a.colF0 = colF0;
   a.rowscale = p->d_rowscale + (size_t)rs * p->J;

@@ -50,6 +50,7 @@ enum UnpackOp : int {
   UNPACK_GRADMU = 2,     // (k+2) eps_{k+1} a_{k+1} - (k-1) eps_k a_{k-1}
   UNPACK_ALPHA = 3,      // i m aA + GRADMU(aB)                   (two inputs)
   UNPACK_VORDIV2UV = 4,  // psi, chi = -a^2 a/(n(n+1)); U = i m chi - GRADMU(psi), V = i m psi + GRADMU(chi)
+  UNPACK_HGRAD = 5,      // i m a and GRADMU(a) from one input    (two column sets)
 };
 
 struct Timing {
@@ -131,7 +132,7 @@ int build_tables(sht_plan *p);
 // scaled per row by rowscale table `rs`.
 int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
                    double2 *F, int ncolF, int colF0, int rs, cudaStream_t s,
-                   const double *const *gcol = nullptr);
+                   const double *const *gcol = nullptr, const double *mul = nullptr, int nmul = 0);
 // F -> grid (two destinations split at nsplit, or column c at ocol[c]),
 // scaled per row by `rs`.
 int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, int ncol,

@@ -12,6 +12,7 @@
 //   synthesis side ("unpack", wa -> internal a, n = m..N+1):
 //     plain      xy_w                              a_n
 //     gradlambda xy_GradLambda_w / GradLon         i m a_n
+//     hgrad      GradLon and GradLat together      i m a_n and R(a)_n (two column sets)
 //     gradmu     xy_GradMu_w / GradLat             R(a)_n = (n+2) eps_{n+1} a_{n+1} - (n-1) eps_n a_{n-1}
 //     alpha      xy_AlphaOptr_w(A,B)               i m aA_n + R(aB)_n
 //     vordiv2uv  calc_VorDiv2UV(vor,div)           psi,chi = -a^2 x/(n(n+1));
@@ -133,6 +134,7 @@ __host__ __device__ constexpr bool unpack_needs(int in, int dn)
 {
   return OP == UNPACK_PLAIN || OP == UNPACK_GRADLAMBDA ? (in == 0 && dn == 0)
        : OP == UNPACK_GRADMU                          ? (in == 0 && dn != 0)
+       : OP == UNPACK_HGRAD                           ? (in == 0)
        : OP == UNPACK_ALPHA                           ? (in == 0 ? dn == 0 : dn != 0)
                                                       : true;  // VORDIV2UV
 }
@@ -210,6 +212,9 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
       v0 = times_im(coef(0, 0), m);
     } else if (OP == UNPACK_GRADMU) {
       v0 = R(0, 0.0);
+    } else if (OP == UNPACK_HGRAD) {
+      v0 = times_im(coef(0, 0), m);
+      v1 = R(0, 0.0);
     } else if (OP == UNPACK_ALPHA) {
       v0 = cadd(times_im(coef(0, 0), m), R(1, 0.0));
     } else {  // UNPACK_VORDIV2UV: input 0 = vor, 1 = div
@@ -221,7 +226,7 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
     }
     const long long row = (long long)(__ldg(a.rowoff + m) + (n - m));
     a.So[row * a.ncolS + b] = v0;
-    if (OP == UNPACK_VORDIV2UV) a.So[row * a.ncolS + a.nb + b] = v1;
+    if (OP == UNPACK_VORDIV2UV || OP == UNPACK_HGRAD) a.So[row * a.ncolS + a.nb + b] = v1;
   }
 }
 
@@ -327,6 +332,7 @@ int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1,
   case UNPACK_GRADMU: run(k_unpack<UNPACK_GRADMU>, unpack_nslots<UNPACK_GRADMU>()); break;
   case UNPACK_ALPHA: run(k_unpack<UNPACK_ALPHA>, unpack_nslots<UNPACK_ALPHA>()); break;
   case UNPACK_VORDIV2UV: run(k_unpack<UNPACK_VORDIV2UV>, unpack_nslots<UNPACK_VORDIV2UV>()); break;
+  case UNPACK_HGRAD: run(k_unpack<UNPACK_HGRAD>, unpack_nslots<UNPACK_HGRAD>()); break;
   default: set_error("unpack: unknown operator"); return SHT_ERR_INVALID_ARG;
   }
   if (e != cudaSuccess) return cuda_fail(e, "k_unpack smem attribute");

@@ -31,6 +31,7 @@ module wa_module_b200
   public :: b200_wa_AlphaOptr_xya, b200_xya_AlphaOptr_wa
   public :: b200_calc_UVCosLat2VorDiv, b200_calc_VorDiv2UV
   public :: b200_wa_Diffuse
+  public :: b200_wa_AlphaOptrProd_xya, b200_xya_HGrad_wa, b200_xya_HGrad_xya
 
   integer, parameter :: SHT_OK = 0
   character(*), parameter :: module_name = 'wa_module_b200'
@@ -165,6 +166,21 @@ module wa_module_b200
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: plan; real(c_double), intent(in) :: vor(*), div(*)
       integer(c_int), value :: nb; real(c_double), intent(out) :: u(*), v(*)
+    end function
+    integer(c_int) function sht_wa_alphaoptr_prod_xya(plan, a, b, q, nb, w) bind(C, name='sht_wa_alphaoptr_prod_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: a(*), b(*), q(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_xya_hgrad_wa(plan, w, nb, glon, glat) bind(C, name='sht_xya_hgrad_wa')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: w(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: glon(*), glat(*)
+    end function
+    integer(c_int) function sht_xya_hgrad_xya(plan, x, nb, glon, glat) bind(C, name='sht_xya_hgrad_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: glon(*), glat(*)
     end function
     integer(c_int) function sht_wa_diffuse(plan, w, nb, coef, dt, filt) bind(C, name='sht_wa_diffuse')
       import :: c_int, c_double, c_ptr
@@ -403,5 +419,29 @@ contains
     real(DP), intent(in) :: coef(:), dt, w_Filter(:)
     call check(sht_wa_diffuse(plan, wa, int(size(wa, 2), c_int), coef, real(dt, c_double), w_Filter), 'wa_Diffuse')
   end subroutine b200_wa_Diffuse
+
+  !> wa_AlphaOptr_xya(A Q, B Q), products formed in the longitude transform
+  !> (dynamics/hspm_vfvm/HBEBaroc_hspm_vfvm_mod.f90:160-165, Q = H cos(phi) T)
+  function b200_wa_AlphaOptrProd_xya(xya_A, xya_B, xya_Q)
+    real(DP), intent(in) :: xya_A(:,:,:), xya_B(:,:,:), xya_Q(:,:,:)
+    real(DP) :: b200_wa_AlphaOptrProd_xya(lm, size(xya_A, 3))
+    call check(sht_wa_alphaoptr_prod_xya(plan, xya_A, xya_B, xya_Q, int(size(xya_A, 3), c_int), &
+         b200_wa_AlphaOptrProd_xya), 'wa_AlphaOptrProd_xya')
+  end function b200_wa_AlphaOptrProd_xya
+
+  !> xya_GradLon_wa and xya_GradLat_wa of one spectrum, one synthesis
+  subroutine b200_xya_HGrad_wa(wa, xya_GradLon, xya_GradLat)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP), intent(out) :: xya_GradLon(:,:,:), xya_GradLat(:,:,:)
+    call check(sht_xya_hgrad_wa(plan, wa, int(size(wa, 2), c_int), xya_GradLon, xya_GradLat), 'xya_HGrad_wa')
+  end subroutine b200_xya_HGrad_wa
+
+  !> xya_GradLon_wa(wa_xya(T)), xya_GradLat_wa(wa_xya(T)): the Redi/GM tracer
+  !> gradients before 1/RPlanet (physics/lphys/LPhys_RediGM_hspm_vfvm_mod.f90:432-440)
+  subroutine b200_xya_HGrad_xya(xya, xya_GradLon, xya_GradLat)
+    real(DP), intent(in) :: xya(:,:,:)
+    real(DP), intent(out) :: xya_GradLon(:,:,:), xya_GradLat(:,:,:)
+    call check(sht_xya_hgrad_xya(plan, xya, int(size(xya, 3), c_int), xya_GradLon, xya_GradLat), 'xya_HGrad_xya')
+  end subroutine b200_xya_HGrad_xya
 
 end module wa_module_b200

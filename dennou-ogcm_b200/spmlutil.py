@@ -44,6 +44,7 @@ _G2S = ["sht_wa_xya", "sht_xya_wa", "sht_wa_divlambda_xya", "sht_wa_divmu_xya",
         "sht_avrlonlat_xya", "sht_intlonlat_xya", "sht_ya_avrlon_xya", "sht_ya_intlon_xya"]
 _TWO_IN = ["sht_wa_alphaoptr_xya", "sht_xya_alphaoptr_wa"]
 _TWO_IO = ["sht_uvcoslat2vordiv", "sht_vordiv2uv"]
+_ONE_IN_TWO_OUT = ["sht_xya_hgrad_wa", "sht_xya_hgrad_xya"]
 
 
 class SpmlError(RuntimeError):
@@ -93,6 +94,11 @@ def load_library(path: str | None = None):
     for name in _TWO_IO:
         for suf in ("", "_dev"):
             getattr(lib, name + suf).argtypes = [_VP, _VP, _VP, ctypes.c_int, _VP, _VP]
+    for name in _ONE_IN_TWO_OUT:
+        for suf in ("", "_dev"):
+            getattr(lib, name + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, _VP]
+    for suf in ("", "_dev"):
+        getattr(lib, "sht_wa_alphaoptr_prod_xya" + suf).argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int, _VP]
     for suf in ("", "_dev"):
         getattr(lib, "sht_wa_diffuse" + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
     lib.sht_roundtrip_diffuse_dev.argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
@@ -343,6 +349,24 @@ class SpmlUtil:
 
     wa_AlphaOptr_xya = w_AlphaOptr_xy
     xya_AlphaOptr_wa = xy_AlphaOptr_w
+
+    def w_AlphaOptrProd_xy(self, xy_A, xy_B, xy_Q):
+        """w_AlphaOptr_xy(A Q, B Q), the products formed inside the longitude
+        transform (HBEBaroc_hspm_vfvm_mod.f90:160-165, Q = H cos(phi) T)."""
+        return self._run("sht_wa_alphaoptr_prod_xya", [xy_A, xy_B, xy_Q], "spec")
+
+    def xy_HGrad_w(self, w):
+        """-> (xy_GradLon_w(w), xy_GradLat_w(w)) in one synthesis."""
+        return self._run("sht_xya_hgrad_wa", [w], "grid", nout=2)
+
+    def xy_HGrad_xy(self, xy):
+        """-> (xy_GradLon_w(w_xy(T)), xy_GradLat_w(w_xy(T))), the Redi/GM tracer
+        gradients before the 1/radius factor (LPhys_RediGM_hspm_vfvm_mod.f90:432-440)."""
+        return self._run("sht_xya_hgrad_xya", [xy], "grid", nout=2)
+
+    wa_AlphaOptrProd_xya = w_AlphaOptrProd_xy
+    xya_HGrad_wa = xy_HGrad_w
+    xya_HGrad_xya = xy_HGrad_xy
 
     def calc_UVCosLat2VorDiv(self, xy_UCosLat, xy_VCosLat):
         """-> (w_Vor, w_Div) (SpmlUtil_mod.f90:299-314, 342-368)."""

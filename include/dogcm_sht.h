@@ -162,6 +162,27 @@ SHT_API int sht_wa_alphaoptr_xya(sht_plan *plan, const double *xya_a, const doub
 SHT_API int sht_xya_alphaoptr_wa(sht_plan *plan, const double *wa_a, const double *wa_b,
                          int nb, double *xya);
 
+/* w_AlphaOptr_xy(A Q, B Q) with the point-by-point products formed inside the
+ * longitude transform: the horizontal tracer flux divergence of the thickness
+ * equation, where Q = H cos(phi) T multiplies both velocity components
+ * (dynamics/hspm_vfvm/HBEBaroc_hspm_vfvm_mod.f90:160-165).  xya_q holds one grid per level, like
+ * xya_a and xya_b. */
+SHT_API int sht_wa_alphaoptr_prod_xya(sht_plan *plan, const double *xya_a, const double *xya_b,
+                              const double *xya_q, int nb, double *wa);
+
+/* xy_GradLon_w and xy_GradLat_w of the same spectrum in one synthesis
+ * (SpmlUtil_mod.f90:114-115): both gradients share the staged spectral
+ * entries and the Legendre and longitude passes run over 2 nb columns. */
+SHT_API int sht_xya_hgrad_wa(sht_plan *plan, const double *wa, int nb, double *xya_lon,
+                     double *xya_lat);
+
+/* The Redi/GM tracer gradients, xy_GradLon_w(w_xy(T)) and
+ * xy_GradLat_w(w_xy(T)) (physics/lphys/LPhys_RediGM_hspm_vfvm_mod.f90:432-440),
+ * grid to grid without a spectral array on the caller's side.  Like the
+ * SPMODEL functions, no 1/radius factor is applied. */
+SHT_API int sht_xya_hgrad_xya(sht_plan *plan, const double *xya, int nb, double *xya_lon,
+                      double *xya_lat);
+
 /* calc_UVCosLat2VorDiv: Vor = H(V cos, -U cos), Div = H(U cos, V cos)
  * (SpmlUtil_mod.f90:299-314, 342-368). Inputs are U cos phi and V cos phi. */
 SHT_API int sht_uvcoslat2vordiv(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
@@ -206,6 +227,12 @@ SHT_API int sht_wa_alphaoptr_xya_dev(sht_plan *plan, const double *xya_a, const 
                              int nb, double *wa);
 SHT_API int sht_xya_alphaoptr_wa_dev(sht_plan *plan, const double *wa_a, const double *wa_b,
                              int nb, double *xya);
+SHT_API int sht_wa_alphaoptr_prod_xya_dev(sht_plan *plan, const double *xya_a, const double *xya_b,
+                                  const double *xya_q, int nb, double *wa);
+SHT_API int sht_xya_hgrad_wa_dev(sht_plan *plan, const double *wa, int nb, double *xya_lon,
+                         double *xya_lat);
+SHT_API int sht_xya_hgrad_xya_dev(sht_plan *plan, const double *xya, int nb, double *xya_lon,
+                          double *xya_lat);
 SHT_API int sht_uvcoslat2vordiv_dev(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
                             int nb, double *wa_vor, double *wa_div);
 SHT_API int sht_vordiv2uv_dev(sht_plan *plan, const double *wa_vor, const double *wa_div,

@@ -61,6 +61,17 @@ def test_calls_on_null_plan_fail_cleanly():
     assert b"not initialised" in lib.sht_last_error()
 
 
+def test_fused_clients_check_arguments_on_the_host():
+    """The product-epilogue and gradient entry points reject a null plan and
+    null arrays before any device work."""
+    lib = pkg().load_library()
+    buf = (ctypes.c_double * 8)()
+    assert lib.sht_wa_alphaoptr_prod_xya(None, buf, buf, buf, 1, buf) == 3
+    assert lib.sht_wa_alphaoptr_prod_xya_dev(None, buf, buf, buf, 1, buf) == 3
+    assert lib.sht_xya_hgrad_wa(None, buf, 1, buf, buf) == 3
+    assert lib.sht_xya_hgrad_xya_dev(None, buf, 1, buf, buf) == 3
+
+
 def test_init_without_device_reports_no_device(cuda_available):
     if cuda_available:
         pytest.skip("a CUDA device is present")
