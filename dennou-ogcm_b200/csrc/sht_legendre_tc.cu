@@ -7,15 +7,19 @@
 // column of the data.  Digit s is stored as the BF16 value d_s 2^{-8s}
 // (exact: 8 significant bits and a power-of-two scale), so the product of
 // digits s and t carries its weight 2^{-8(s+t)} by itself.  The pairs with
-// s + t <= 6 are kept (28 MMAs per K step).  Pairs of level L = s + t < 4 go
+// s + t <= 6 are kept (28 MMAs per K step).  Pairs of level L = s + t < 5 go
 // to accumulator L: every such product is an integer multiple of 2^{-8L} of
-// magnitude at most 2^{14-8L}, so the FP32 sum over K <= 256 of at most four
-// pairs stays an exact multiple of at most 2^{24-8L} -- exact.  Levels 4..6
-// share a fifth accumulator; its FP32 rounding is 2^{-24} of a quantity that
-// is itself about 2^{-32} of the result's scale (keeping level 3 apart as well
-// matters: merged from level 3 on, the rounding reached 3e-11 of a field's
-// maximum on cancelling sums).  The five accumulators are summed in FP64
-// (smallest first) and scaled by the two exponents (the Ozaki error-free
+// magnitude at most 2^{14-8L}, so the FP32 sum over K <= 256 of the L + 1
+// pairs of levels 0..3 stays an exact multiple of at most 2^{24-8L} -- exact;
+// level 4 is exact for K <= 204 and beyond that rounds only where its partial
+// sums pass 4/5 of their bound.  Levels 5 and 6 share a sixth accumulator.
+// Each MMA's sum is rounded into the FP32 accumulator, and nothing is assumed
+// about the direction, so the error of a shared accumulator is bounded by the
+// number of MMAs into it times the ulp of its largest level: levels 4..6 in one
+// accumulator reached 1.3e-11 of a field's maximum at T341 (K = 172..256,
+// 288 roundings at 2^{-45} of the result's scale), levels 3..6 reached 3e-11
+// at T42; from level 5 on it is 2^{-52} per rounding.  The six accumulators
+// are summed in FP64 (smallest first) and scaled by the two exponents (the Ozaki error-free
 // splitting, Ozaki-Ogita-Oishi-Rump, Numer. Algorithms 59 (2012)).  Each
 // operand keeps 56 bits (the digit residual is below 2^-56 of its row or column
 // maximum), and the dropped products are below 2^-62.
@@ -29,7 +33,7 @@
 //   * The data digits of chunk u+1 (and its table digits) are written into
 //     the other of two shared-memory stages while the tensor core runs the
 //     asynchronous MMAs of chunk u, issued by one thread.
-//   * When a segment's last chunk completes, all threads read its five TMEM
+//   * When a segment's last chunk completes, all threads read its six TMEM
 //     accumulators, 16 columns at a time (the two warp halves take alternate
 //     groups), and recombine them in FP64.
 //   * M = 128 data columns (re/im of 64 field-levels; TMEM lane = column).
@@ -51,8 +55,8 @@ namespace sht {
 namespace {
 
 constexpr int kS = 7;                      // digits per operand
-constexpr int kAcc = 5;                    // TMEM accumulators: levels 0, 1, 2, 3 and 4..6
-constexpr int kSeg = 96;                   // analysis: output columns per segment (kAcc x kSeg <= 512 TMEM columns)
+constexpr int kAcc = 6;                    // TMEM accumulators: levels 0, 1, 2, 3, 4 and 5..6
+constexpr int kSeg = 80;                   // analysis: output columns per segment (kAcc x kSeg <= 512 TMEM columns)
 constexpr int kSegInv = 64;                // synthesis with output staging: Gauss rows per segment
 constexpr int kStg = 2 * 16 + 2;           // doubles per field-level row of the synthesis output staging
 constexpr int kKC = 32;                    // K per chunk (2 MMA K-steps of 16)
@@ -453,7 +457,7 @@ __device__ void readout(const TcArgs &a, const Sub &s, int col0, const Smem &sm,
       }
     } else if (a.seg_inv != kSegInv) {
       // even-degree sums at F[m][col][jh], odd at F[m][col][JH + jh], straight
-      // from the registers (no room for the staging next to 96-row segments)
+      // from the registers (no room for the staging next to kSeg-row segments)
       if (!valid) continue;
       const int *ge = a.texp + (s.m * 2 + s.p) * a.JH;
       double *Fc = reinterpret_cast<double *>(a.Fo + ((long long)s.m * a.ncol + b) * a.J) + part + 2 * s.p * a.JH;

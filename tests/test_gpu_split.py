@@ -119,3 +119,56 @@ def test_split_rejects_grids_it_does_not_cover(plan_cache):
         assert ei.value.status == 2
     finally:
         gpu.set_precision(P.SHT_PREC_FP64)
+
+
+def _trel(a, b) -> float:
+    """relerr of two device tensors, on the device (fields = leading axis)."""
+    a = a.reshape(a.shape[0], -1)
+    b = b.reshape(b.shape[0], -1)
+    den = b.abs().amax(dim=1)
+    den = den.masked_fill(den == 0, 1.0)
+    return float(((a - b).abs().amax(dim=1) / den).max())
+
+
+def _config_results(gpu, w, coef):
+    """Every C2/C4 quantity of one precision, on device arrays: synthesis,
+    analysis round trip, both gradients, AlphaOptr of two grids, and the
+    backward-Euler diffusion round trip."""
+    import torch
+    g = gpu.xya_wa(w)
+    back = gpu.wa_xya(g)
+    glon, glat = gpu.xy_HGrad_w(w)
+    alpha = gpu.wa_AlphaOptr_xya(g, glat)
+    d = g.clone()
+    gpu.roundtrip_diffuse_(d, coef, 1.0)
+    torch.cuda.synchronize()
+    return dict(g=g, back=back, glon=glon, glat=glat, alpha=alpha, diffused=d)
+
+
+@pytest.mark.parametrize("cfg", ["C2", "C4"])
+def test_config_full_batch_split_vs_fp64(cfg):
+    """C2 (T170, 60 x 12, p = 1.5) and C4 (T341, 60 x 16, p = 2, Ord-8
+    diffusion with dt nu = 1e-3): the whole batch in split precision against
+    the FP64 GPU path, which the oracle pins at these truncations on small
+    batches; the round trip against the identity."""
+    import torch
+    P, W = pkg(), workloads()
+    c = W.CONFIGS[cfg]
+    I, J, N = W.GRIDS[c["grid"]]
+    nb = c["levels"] * c["fields"]
+    dev = torch.device("cuda")
+    gpu = P.SpmlUtil(I, J, 1, N, None, 6.371e6)
+    try:
+        w = W.seeded_spectra_torch(N, nb, c["power"], dev)
+        coef = torch.from_numpy(W.diffusion_coef(N, 8, 1e-3)).to(dev)
+        ref = _config_results(gpu, w, coef)
+        gpu.set_precision(P.SHT_PREC_SPLIT)
+        try:
+            got = _config_results(gpu, w, coef)
+        finally:
+            gpu.set_precision(P.SHT_PREC_FP64)
+        for k in ref:
+            assert _trel(got[k], ref[k]) < TOL, k
+        assert _trel(got["back"], w) < TOL and _trel(ref["back"], w) < TOL
+    finally:
+        gpu.final()
