@@ -317,6 +317,8 @@ def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
              max(_rel(lon.cpu().numpy(), rlon.cpu().numpy()), _rel(lat.cpu().numpy(), rlat.cpu().numpy())))):
         tf, tu = timeit(fused), timeit(unfused)
         out[name] = {"fused_ms": tf, "unfused_ms": tu, "speedup": tu / tf, "relerr_vs_unfused": err}
+    # the same analysis without the products: what the product epilogue adds
+    out["alphaoptr_prod"]["alphaoptr_without_products_ms"] = timeit(lambda: sht.w_AlphaOptr_xy(A, B))
     return out
 
 

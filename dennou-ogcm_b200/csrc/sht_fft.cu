@@ -129,6 +129,7 @@ struct FftArgs {
   const double *mul;
   int nmul;
   int mul_staged;  // factor rows staged with the tile (else read in the first pass)
+  int mul_pair;    // columns c and nsplit + c share a factor: visit them one after the other
 };
 
 // Shared-memory plan of one thread block: the twiddle tables (2 NC entries),
@@ -177,7 +178,10 @@ __device__ __forceinline__ void load_twiddles(const FftArgs &a, double2 *stw, do
 // Forward transform, persistent over tiles (field-level, JT latitude rows).
 // Tile t+gridDim.x streams into one buffer (cp.async, 16 bytes per thread per
 // copy) while tile t is transformed in place in the other.
-template <int A, int B, int NT>
+// MUL: 0 plain, 1 product with the factor rows staged beside the tile, 2
+// product with the factor read through the read-only cache (issued before the
+// wait for the tile, so that both loads are in flight together).
+template <int A, int B, int NT, int MUL>
 __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
 {
   using S = FftShape<A, B, NT>;
@@ -195,7 +199,8 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
   const long long mstride = (long long)a.ncolF * a.J;
 
   auto issue = [&](long long t, double2 *buf) {
-    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
+    const int c2 = (int)(t / ntile), h0 = (int)(t - (long long)c2 * ntile) * JTh;
+    const int col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
     const double *gb = a.gcol ? a.gcol[col]
                      : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
     const double2 *src = reinterpret_cast<const double2 *>(gb);
@@ -206,7 +211,7 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
       const int j = rr < JTh ? a.JH + jh : a.JH - 1 - jh;
       if (jh < a.JH) cp_async16(buf + rr * NCp + c, src + (long long)j * NC + c, true);
     }
-    if (a.mul && a.mul_staged) {  // the factor's rows, in the second half of the buffer
+    if (MUL == 1) {  // the factor's rows, in the second half of the buffer
       const double2 *fsrc = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ);
 #pragma unroll 4
       for (int q = tid; q < JT * NC; q += NT) {
@@ -225,22 +230,29 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
     double2 *cur = sm + (it & 1) * bufe;
     if (t + gridDim.x < ntot) issue(t + gridDim.x, sm + ((it + 1) & 1) * bufe);
     cp_async_commit();
+
+    const int c2 = (int)(t / ntile), h0 = (int)(t - (long long)c2 * ntile) * JTh;
+    const int col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
+    const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
+    const bool valid = jh < a.JH;
+    double2 f[MUL == 2 ? R1 : 1];
+    if (MUL == 2) {
+      const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)j * NC;
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) f[n1] = valid ? __ldg(frow + R2 * n1 + u) : make_double2(0.0, 0.0);
+    }
     cp_async_wait<1>();
     __syncthreads();
 
-    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
-    const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
-    const bool valid = jh < a.JH;
     // pass A: R1-point DFTs over elements strided by R2
     double2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? cur[r * NCp + R2 * n1 + u] : make_double2(0.0, 0.0);
-    if (a.mul && valid) {
-      const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)j * NC;
+    if (MUL != 0) {
 #pragma unroll
       for (int n1 = 0; n1 < R1; ++n1) {
-        const double2 f = a.mul_staged ? cur[JT * NCp + r * NCp + R2 * n1 + u] : __ldg(frow + R2 * n1 + u);
-        v[n1] = make_double2(v[n1].x * f.x, v[n1].y * f.y);
+        const double2 q = MUL == 1 ? cur[JT * NCp + r * NCp + R2 * n1 + u] : f[MUL == 2 ? n1 : 0];
+        v[n1] = make_double2(v[n1].x * q.x, v[n1].y * q.y);
       }
     }
     __syncthreads();  // the staged tile is consumed; the buffer is reused below
@@ -492,10 +504,15 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s
   using S = FftShape<A, B, kFftThreads>;
   int bufe = S::buf_elems(p->N);
   FftArgs a = args;
-  if (!inverse && a.mul) {  // room for the factor's tile beside the data tile, where it fits
+  if (!inverse && a.mul) {
+    // room for the factor's tile beside the data tile, where that costs no
+    // resident block (otherwise the first pass reads the factor through the
+    // read-only cache)
     const int two = (2 * S::JT * S::NCp + 7) & ~7;
     const int want = bufe > two ? bufe : two;
-    a.mul_staged = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)want) <= 227 * 1024;
+    auto bytes = [](int e) { return sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)e); };
+    auto per_sm = [](size_t b) { return (int)((228 * 1024) / (b + 1024)); };
+    a.mul_staged = bytes(want) <= 227 * 1024 && per_sm(bytes(want)) >= per_sm(bytes(bufe));
     if (a.mul_staged) bufe = want;
   }
   const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)bufe);
@@ -509,7 +526,9 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s
     kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(a, bufe);
   };
   if (inverse) go(k_fft_inv<A, B, kFftThreads>);
-  else go(k_fft_fwd<A, B, kFftThreads>);
+  else if (!a.mul) go(k_fft_fwd<A, B, kFftThreads, 0>);
+  else if (a.mul_staged) go(k_fft_fwd<A, B, kFftThreads, 1>);
+  else go(k_fft_fwd<A, B, kFftThreads, 2>);
   if (e != cudaSuccess) return cuda_fail(e, "fft smem attribute");
   count_launch();
   e = cudaGetLastError();
@@ -551,6 +570,9 @@ int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int ns
   a.gcol = gcol;
   a.mul = mul;
   a.nmul = nmul > 0 ? nmul : 1;
+  // the two inputs' tiles of one level run back to back, so the level's
+  // factor grid comes from L2 the second time
+  a.mul_pair = (mul && !gcol && g1 && ncol == 2 * nsplit) ? 1 : 0;
   a.g0 = g0; a.g1 = g1 ? g1 : g0; a.nsplit = nsplit; a.ncol = ncol;
   a.F = F; a.ncolF = ncolF; a.colF0 = colF0;
   a.rowscale = p->d_rowscale + (size_t)rs * p->J;

@@ -25,6 +25,9 @@
 //   * The first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current).  Make
 //     that first call before any stream capture begins.
+//   * In split precision the plan's digit tables must exist already: the first
+//     split-precision call of an ordinary entry point allocates them.  Until
+//     then this entry point refuses (SHT_ERR_INVALID_ARG) instead of allocating.
 #include "sht_internal.h"
 
 #include <cstdio>
@@ -93,6 +96,13 @@ extern "C" SHT_API int sht_wa_xya_dev_noalloc(sht_plan *p, const double *xya, in
     return SHT_ERR_TOO_LARGE;
   }
   std::lock_guard<std::mutex> lk(p->mtx);
+  if (p->precision == SHT_PREC_SPLIT && !p->tc_tables) {
+    // the split kernel's digit tables are allocated by the first split-precision
+    // transform of a plan; this entry point must not be the one to do it
+    set_error("noalloc: split precision needs the plan's digit tables, which the first split-precision "
+              "call of an ordinary entry point allocates; make one such call first, or use FP64");
+    return SHT_ERR_INVALID_ARG;
+  }
   int prev = -1;
   cudaGetDevice(&prev);
   if (prev != p->device && cudaSetDevice(p->device) != cudaSuccess) {

@@ -268,7 +268,10 @@ SHT_API int sht_roundtrip_diffuse_dev(sht_plan *plan, double *xya, int nb, const
  * calls share that array, so calls that overlap on the GPU race: order them
  * on one stream.  The first call on each device looks up the array's address
  * (cudaGetSymbolAddress), so make it before any stream capture.  The plan
- * must already exist (sht_init allocates its tables). */
+ * must already exist (sht_init allocates its tables); in split precision,
+ * so must its digit tables, which the plan's first split-precision call of an
+ * ordinary entry point allocates (until then this returns
+ * SHT_ERR_INVALID_ARG). */
 SHT_API int sht_wa_xya_dev_noalloc(sht_plan *plan, const double *xya, int nb, double *wa);
 SHT_API unsigned long long sht_noalloc_scratch_bytes(void);
 

@@ -79,3 +79,36 @@ def test_noalloc_rejects_batches_beyond_the_fixed_scratch():
         assert b"limit" in lib.sht_last_error()
     finally:
         sht.final()
+
+
+def test_noalloc_split_precision_needs_tables_built_elsewhere():
+    """In split precision the digit tables are allocated by the plan's first
+    split call of an ordinary entry point; before that the allocation-free
+    entry point refuses instead of allocating them, and afterwards it matches
+    the ordinary entry point on two calls in a row."""
+    import torch
+
+    P, W = pkg(), workloads()
+    lib = _lib()
+    I, J, N = W.GRIDS["T42"]
+    nb = 20
+    sht = P.SpmlUtil(I, J, nb, N, None, 1.0)
+    try:
+        stream = torch.cuda.current_stream()
+        assert lib.sht_set_stream(sht._h, VP(stream.cuda_stream)) == 0
+        w = torch.from_numpy(W.seeded_spectra(N, nb, 1.5, seed=7)).cuda()
+        grid = sht.xya_wa(w)
+        out = torch.zeros((nb, (N + 1) ** 2), dtype=torch.float64, device="cuda")
+        sht.set_precision(P.SHT_PREC_SPLIT)
+        st = lib.sht_wa_xya_dev_noalloc(sht._h, VP(grid.data_ptr()), nb, VP(out.data_ptr()))
+        assert st == 1 and b"digit tables" in lib.sht_last_error()
+        ref = torch.empty_like(out)
+        for _ in range(2):
+            out.fill_(float("nan"))
+            assert lib.sht_wa_xya_dev(sht._h, VP(grid.data_ptr()), nb, VP(ref.data_ptr())) == 0
+            assert lib.sht_wa_xya_dev_noalloc(sht._h, VP(grid.data_ptr()), nb, VP(out.data_ptr())) == 0
+            torch.cuda.synchronize()
+            assert relerr(out.cpu().numpy(), ref.cpu().numpy()) < TOL
+    finally:
+        sht.set_precision(P.SHT_PREC_FP64)
+        sht.final()
