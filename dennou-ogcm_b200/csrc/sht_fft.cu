@@ -266,7 +266,8 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
     }
     __syncthreads();
 
-    // pass B: R2-point DFTs
+    // pass B: R2-point DFTs; this thread then holds Z_m for
+    // m = k1 + R1 k2, k1 = u + T s, i.e. m = u + T q with q = s + NS k2
     double2 z[NS][R2];
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
@@ -275,35 +276,31 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
       for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
       dft_reg<B, false>(z[s]);
     }
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-#pragma unroll
-      for (int k2 = 0; k2 < R2; ++k2) srow[(u + T * s) + R1 * k2] = z[s][brev<B>(k2)];
-    __syncthreads();
+    // Z_{NC-m}: for u != 0 it sits in lane T - u of the same row at
+    // (s, k2) -> (NS-1-s, R2-1-k2); for u = 0 in this thread, at (0, -k2 mod R2)
+    // when s = 0 and at (NS-s, R2-1-k2) otherwise
+    const int lane = tid & 31, partner = (lane & ~(T - 1)) | ((T - u) & (T - 1));
+    __syncthreads();  // every row's pass-B reads are done; the staging below overwrites them
 
-    // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I}
+    // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I},
+    // written transposed (m-major) for the output runs
     const double sc = valid ? __ldg(a.rowscale + j) : 0.0;
-    double2 xo[R1];
 #pragma unroll
     for (int q = 0; q < R1; ++q) {
-      const int m = u + T * q;
-      xo[q] = make_double2(0.0, 0.0);
+      const int s = q % NS, k2 = q / NS, m = u + T * q;
+      const double2 src = z[NS - 1 - s][brev<B>(R2 - 1 - k2)];
+      double2 zc;
+      zc.x = __shfl_sync(0xffffffffu, src.x, partner);
+      zc.y = __shfl_sync(0xffffffffu, src.y, partner);
+      if (u == 0) zc = (s == 0) ? z[0][brev<B>((R2 - k2) & (R2 - 1))] : z[s == 0 ? 0 : NS - s][brev<B>(R2 - 1 - k2)];
       if (m <= a.N) {
-        const int mm = (NC - m) & (NC - 1);
-        const double2 zm = srow[m], zc = srow[mm];
+        const double2 zm = z[s][brev<B>(k2)];
         const double er = 0.5 * (zm.x + zc.x), ei = 0.5 * (zm.y - zc.y);
         const double dr = 0.5 * (zm.x - zc.x), di = 0.5 * (zm.y + zc.y);
         const double2 w = stwI[m];
         const double tr = w.x * dr - w.y * di, ti = w.x * di + w.y * dr;
-        xo[q] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
+        cur[m * JTp + r] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
       }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int q = 0; q < R1; ++q) {
-      const int m = u + T * q;
-      if (m <= a.N) cur[m * JTp + r] = xo[q];
     }
     __syncthreads();
 
@@ -375,20 +372,47 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
       return make_double2(e.x + sgn * o.x, e.y + sgn * o.y);
     };
 
-    // real pack: Z_k = (X_k + Y_k) + i w^k (X_k - Y_k), Y_k = conj X_{NC-k}, w = e^{+2 pi i/I}
+    // real pack: Z_k = (X_k + Y_k) + i w^k (X_k - Y_k), Y_k = conj X_{NC-k}, w = e^{+2 pi i/I}.
+    // Up to R1 = 16 this thread reads X_k for k = R2 n1 + u only, and X_{NC-k}
+    // comes from lane T - u of the same row at n1' = R1-1-n1 (u != 0) or from
+    // this thread at n1' = -n1 mod R1 (u = 0).  At R1 = 32 the extra registers
+    // would spill, so both are read from shared memory.
+    constexpr bool kShfl = R1 <= 16;
+    double2 xk[kShfl ? R1 : 1];
+    if constexpr (kShfl) {
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const int k = R2 * n1 + u;
+        xk[n1] = make_double2(0.0, 0.0);
+        if (k <= a.N) {
+          xk[n1] = gm(k);
+          if (k == 0) xk[n1].y = 0.0;
+        }
+      }
+    }
+    const int lane = tid & 31, partner = (lane & ~(T - 1)) | ((T - u) & (T - 1));
     double2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) {
       const int k = R2 * n1 + u;
       double2 X = make_double2(0.0, 0.0), Y = make_double2(0.0, 0.0);
-      if (k <= a.N) {
-        X = gm(k);
-        if (k == 0) X.y = 0.0;
-      }
-      const int kk = NC - k;
-      if (k > 0 && kk <= a.N) {
-        const double2 q = gm(kk);
+      if constexpr (kShfl) {
+        X = xk[n1];
+        double2 q;
+        q.x = __shfl_sync(0xffffffffu, xk[R1 - 1 - n1].x, partner);
+        q.y = __shfl_sync(0xffffffffu, xk[R1 - 1 - n1].y, partner);
+        if (u == 0) q = (n1 == 0) ? make_double2(0.0, 0.0) : xk[(R1 - n1) & (R1 - 1)];
         Y = make_double2(q.x, -q.y);
+      } else {
+        if (k <= a.N) {
+          X = gm(k);
+          if (k == 0) X.y = 0.0;
+        }
+        const int kk = NC - k;
+        if (k > 0 && kk <= a.N) {
+          const double2 q = gm(kk);
+          Y = make_double2(q.x, -q.y);
+        }
       }
       const double2 wI = stwI[k];
       const double wr = wI.x, wi = -wI.y;
