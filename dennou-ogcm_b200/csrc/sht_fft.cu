@@ -128,25 +128,22 @@ struct FftArgs {
   // grid field mul + (col mod nmul) I J before the transform
   const double *mul;
   int nmul;
-  int mul_staged;  // factor rows staged with the tile (else read in the first pass)
   int mul_pair;    // columns c and nsplit + c share a factor: visit them one after the other
 };
 
 // Shared-memory plan of one thread block: the twiddle tables (2 NC entries),
-// then two buffers, each large enough for a staged input tile and, in place,
-// for every later stage of that tile.
+// then the tile buffers (two in the inverse, whose next tile's Fourier runs
+// stream into one while the other is transformed; one in the forward, whose
+// rows go from global memory straight to registers), each large enough for
+// the in-place DFT rows and the m-major staging.
 template <int A, int B, int NT>
 struct FftShape {
   static constexpr int R1 = 1 << A, R2 = 1 << B, NC = R1 * R2, T = R2, JT = NT / T;
   static constexpr int RS = fft_row_stride<R1, R2, T>();
   static constexpr int JTp = fft_out_stride(JT, T);
-  // staged grid rows are padded so that the 8/T rows of one 8-lane phase of a
-  // 16-byte access fall into distinct bank groups
-  static constexpr int NCp = NC + (T < 8 ? T : 0);
-  static int buf_elems(int N)  // double2 per buffer
+  static int buf_elems(int N)  // double2 per buffer: the in-place DFT rows and the m-major staging
   {
-    int b = JT * NCp;
-    b = b > JT * RS ? b : JT * RS;
+    int b = JT * RS;
     b = b > (N + 1) * JTp ? b : (N + 1) * JTp;
     return (b + 7) & ~7;
   }
@@ -175,149 +172,125 @@ __device__ __forceinline__ void load_twiddles(const FftArgs &a, double2 *stw, do
   }
 }
 
-// Forward transform, persistent over tiles (field-level, JT latitude rows).
-// Tile t+gridDim.x streams into one buffer (cp.async, 16 bytes per thread per
-// copy) while tile t is transformed in place in the other.
-// MUL: 0 plain, 1 product with the factor rows staged beside the tile, 2
-// product with the factor read through the read-only cache (issued before the
-// wait for the tile, so that both loads are in flight together).
-template <int A, int B, int NT, int MUL>
-__global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a, int bufe)
+// One forward tile after its rows are in registers (v: this thread's R1
+// elements of row r, stride R2, already multiplied by any factor): the
+// four-step DFT, the real unpack and the Gs/Ga output runs.  cur is the
+// block's tile buffer, free for reuse on entry.
+template <int A, int B, int NT>
+__device__ __forceinline__ void fwd_tile(const FftArgs &a, double2 (&v)[1 << A], double2 *cur, const double2 *stw,
+                                         const double2 *stwI, int col, int h0, int j, bool valid)
 {
   using S = FftShape<A, B, NT>;
-  constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT, RS = S::RS, JTp = S::JTp, NCp = S::NCp;
+  constexpr int R1 = S::R1, R2 = S::R2, T = S::T, JT = S::JT, RS = S::RS, JTp = S::JTp;
   constexpr int NS = R1 / T;
-  extern __shared__ __align__(16) double2 smem_all[];
-  double2 *stw = smem_all, *stwI = smem_all + NC, *sm = smem_all + 2 * NC;
-  load_twiddles<T, NC, NT>(a, stw, stwI);
+  constexpr int JTh = JT / 2;
+  const int tid = threadIdx.x, r = tid / T, u = tid % T;
+  const long long mstride = (long long)a.ncolF * a.J;
+  dft_reg<A, false>(v);
+  double2 *srow = cur + r * RS;
+#pragma unroll
+  for (int k1 = 0; k1 < R1; ++k1) {
+    double2 y = v[brev<A>(k1)];
+    if (k1 != 0) y = cmul(y, stw[k1 * T + u]);
+    srow[u * (R1 + 1) + k1] = y;
+  }
+  __syncthreads();
 
-  constexpr int JTh = JT / 2;  // mirrored row pairs per tile
+  // pass B: R2-point DFTs; this thread then holds Z_m for
+  // m = k1 + R1 k2, k1 = u + T s, i.e. m = u + T q with q = s + NS k2
+  double2 z[NS][R2];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const int k1 = u + T * s;
+#pragma unroll
+    for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
+    dft_reg<B, false>(z[s]);
+  }
+  // Z_{NC-m}: for u != 0 it sits in lane T - u of the same row at
+  // (s, k2) -> (NS-1-s, R2-1-k2); for u = 0 in this thread, at (0, -k2 mod R2)
+  // when s = 0 and at (NS-s, R2-1-k2) otherwise
+  const int lane = tid & 31, partner = (lane & ~(T - 1)) | ((T - u) & (T - 1));
+  __syncthreads();  // every row's pass-B reads are done; the staging below overwrites them
+
+  // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I},
+  // written transposed (m-major) for the output runs
+  const double sc = valid ? __ldg(a.rowscale + j) : 0.0;
+#pragma unroll
+  for (int q = 0; q < R1; ++q) {
+    const int s = q % NS, k2 = q / NS, m = u + T * q;
+    const double2 src = z[NS - 1 - s][brev<B>(R2 - 1 - k2)];
+    double2 zc;
+    zc.x = __shfl_sync(0xffffffffu, src.x, partner);
+    zc.y = __shfl_sync(0xffffffffu, src.y, partner);
+    if (u == 0) zc = (s == 0) ? z[0][brev<B>((R2 - k2) & (R2 - 1))] : z[s == 0 ? 0 : NS - s][brev<B>(R2 - 1 - k2)];
+    if (m <= a.N) {
+      const double2 zm = z[s][brev<B>(k2)];
+      const double er = 0.5 * (zm.x + zc.x), ei = 0.5 * (zm.y - zc.y);
+      const double dr = 0.5 * (zm.x - zc.x), di = 0.5 * (zm.y + zc.y);
+      const double2 w = stwI[m];
+      const double tr = w.x * dr - w.y * di, ti = w.x * di + w.y * dr;
+      cur[m * JTp + r] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
+    }
+  }
+  __syncthreads();
+
+  // runs Gs = north + south at F[m][col][jh], Ga = north - south at F[m][col][JH + jh]
+  const int nh = min(JTh, a.JH - h0);
+  double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + h0;
+  for (int idx = tid; idx < (a.N + 1) * JTh; idx += NT) {
+    const int m = idx / JTh, i = idx - m * JTh;
+    if (i < nh) {
+      const double2 gn = cur[m * JTp + i], gs = cur[m * JTp + JTh + i];
+      Fb[m * mstride + i] = make_double2(gn.x + gs.x, gn.y + gs.y);
+      Fb[m * mstride + a.JH + i] = make_double2(gn.x - gs.x, gn.y - gs.y);
+    }
+  }
+}
+
+// Forward transform, persistent over tiles (field-level, JT latitude rows).
+// Each thread loads its R1 elements of row r (stride R2) from global memory
+// straight into registers; the block's one shared buffer takes the transpose
+// and the output staging.  Staging the tile with cp.async as well, in a
+// second pair of buffers, cost blocks per SM and measured the same at T85 and
+// 7-18 % slower at T170/T341.
+// MUL: 0 plain, 1 product with the factor grid (FftArgs::mul), read the same way.
+template <int A, int B, int NT, int MUL>
+__global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
+{
+  using S = FftShape<A, B, NT>;
+  constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT;
+  extern __shared__ __align__(16) double2 smem_all[];
+  double2 *stw = smem_all, *stwI = smem_all + NC, *cur = smem_all + 2 * NC;
+  load_twiddles<T, NC, NT>(a, stw, stwI);
+  __syncthreads();
+
+  constexpr int JTh = JT / 2;
   const int tid = threadIdx.x, r = tid / T, u = tid % T;
   const int ntile = (a.JH + JTh - 1) / JTh;
   const long long ntot = (long long)a.ncol * ntile;
   const long long IJ = (long long)a.I * a.J;
-  const long long mstride = (long long)a.ncolF * a.J;
-
-  auto issue = [&](long long t, double2 *buf) {
-    const int c2 = (int)(t / ntile), h0 = (int)(t - (long long)c2 * ntile) * JTh;
-    const int col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
-    const double *gb = a.gcol ? a.gcol[col]
-                     : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
-    const double2 *src = reinterpret_cast<const double2 *>(gb);
-#pragma unroll 4
-    for (int q = tid; q < JT * NC; q += NT) {
-      const int rr = q / NC, c = q - rr * NC;
-      const int jh = h0 + (rr % JTh);
-      const int j = rr < JTh ? a.JH + jh : a.JH - 1 - jh;
-      if (jh < a.JH) cp_async16(buf + rr * NCp + c, src + (long long)j * NC + c, true);
-    }
-    if (MUL == 1) {  // the factor's rows, in the second half of the buffer
-      const double2 *fsrc = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ);
-#pragma unroll 4
-      for (int q = tid; q < JT * NC; q += NT) {
-        const int rr = q / NC, c = q - rr * NC;
-        const int jh = h0 + (rr % JTh);
-        const int j = rr < JTh ? a.JH + jh : a.JH - 1 - jh;
-        if (jh < a.JH) cp_async16(buf + JT * NCp + rr * NCp + c, fsrc + (long long)j * NC + c, true);
-      }
-    }
-  };
-
-  long long t = blockIdx.x;
-  if (t < ntot) issue(t, sm);
-  cp_async_commit();
-  for (int it = 0; t < ntot; t += gridDim.x, ++it) {
-    double2 *cur = sm + (it & 1) * bufe;
-    if (t + gridDim.x < ntot) issue(t + gridDim.x, sm + ((it + 1) & 1) * bufe);
-    cp_async_commit();
-
+  for (long long t = blockIdx.x; t < ntot; t += gridDim.x) {
     const int c2 = (int)(t / ntile), h0 = (int)(t - (long long)c2 * ntile) * JTh;
     const int col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
     const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
     const bool valid = jh < a.JH;
-    double2 f[MUL == 2 ? R1 : 1];
-    if (MUL == 2) {
-      const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)j * NC;
-#pragma unroll
-      for (int n1 = 0; n1 < R1; ++n1) f[n1] = valid ? __ldg(frow + R2 * n1 + u) : make_double2(0.0, 0.0);
-    }
-    cp_async_wait<1>();
-    __syncthreads();
-
-    // pass A: R1-point DFTs over elements strided by R2
+    const double *gb = a.gcol ? a.gcol[col]
+                     : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
+    const double2 *src = reinterpret_cast<const double2 *>(gb) + (long long)(valid ? j : 0) * NC;
     double2 v[R1];
 #pragma unroll
-    for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? cur[r * NCp + R2 * n1 + u] : make_double2(0.0, 0.0);
-    if (MUL != 0) {
+    for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? __ldcs(src + R2 * n1 + u) : make_double2(0.0, 0.0);
+    if (MUL == 1) {
+      const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)(valid ? j : 0) * NC;
 #pragma unroll
       for (int n1 = 0; n1 < R1; ++n1) {
-        const double2 q = MUL == 1 ? cur[JT * NCp + r * NCp + R2 * n1 + u] : f[MUL == 2 ? n1 : 0];
+        const double2 q = valid ? __ldg(frow + R2 * n1 + u) : make_double2(0.0, 0.0);
         v[n1] = make_double2(v[n1].x * q.x, v[n1].y * q.y);
       }
     }
-    __syncthreads();  // the staged tile is consumed; the buffer is reused below
-    dft_reg<A, false>(v);
-    double2 *srow = cur + r * RS;
-#pragma unroll
-    for (int k1 = 0; k1 < R1; ++k1) {
-      double2 y = v[brev<A>(k1)];
-      if (k1 != 0) y = cmul(y, stw[k1 * T + u]);
-      srow[u * (R1 + 1) + k1] = y;
-    }
-    __syncthreads();
-
-    // pass B: R2-point DFTs; this thread then holds Z_m for
-    // m = k1 + R1 k2, k1 = u + T s, i.e. m = u + T q with q = s + NS k2
-    double2 z[NS][R2];
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-      const int k1 = u + T * s;
-#pragma unroll
-      for (int n2 = 0; n2 < R2; ++n2) z[s][n2] = srow[n2 * (R1 + 1) + k1];
-      dft_reg<B, false>(z[s]);
-    }
-    // Z_{NC-m}: for u != 0 it sits in lane T - u of the same row at
-    // (s, k2) -> (NS-1-s, R2-1-k2); for u = 0 in this thread, at (0, -k2 mod R2)
-    // when s = 0 and at (NS-s, R2-1-k2) otherwise
-    const int lane = tid & 31, partner = (lane & ~(T - 1)) | ((T - u) & (T - 1));
-    __syncthreads();  // every row's pass-B reads are done; the staging below overwrites them
-
-    // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I},
-    // written transposed (m-major) for the output runs
-    const double sc = valid ? __ldg(a.rowscale + j) : 0.0;
-#pragma unroll
-    for (int q = 0; q < R1; ++q) {
-      const int s = q % NS, k2 = q / NS, m = u + T * q;
-      const double2 src = z[NS - 1 - s][brev<B>(R2 - 1 - k2)];
-      double2 zc;
-      zc.x = __shfl_sync(0xffffffffu, src.x, partner);
-      zc.y = __shfl_sync(0xffffffffu, src.y, partner);
-      if (u == 0) zc = (s == 0) ? z[0][brev<B>((R2 - k2) & (R2 - 1))] : z[s == 0 ? 0 : NS - s][brev<B>(R2 - 1 - k2)];
-      if (m <= a.N) {
-        const double2 zm = z[s][brev<B>(k2)];
-        const double er = 0.5 * (zm.x + zc.x), ei = 0.5 * (zm.y - zc.y);
-        const double dr = 0.5 * (zm.x - zc.x), di = 0.5 * (zm.y + zc.y);
-        const double2 w = stwI[m];
-        const double tr = w.x * dr - w.y * di, ti = w.x * di + w.y * dr;
-        cur[m * JTp + r] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
-      }
-    }
-    __syncthreads();
-
-    // runs Gs = north + south at F[m][col][jh], Ga = north - south at F[m][col][JH + jh]
-    const int nh = min(JTh, a.JH - h0);
-    double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + h0;
-    for (int idx = tid; idx < (a.N + 1) * JTh; idx += NT) {
-      const int m = idx / JTh, i = idx - m * JTh;
-      if (i < nh) {
-        const double2 gn = cur[m * JTp + i], gs = cur[m * JTp + JTh + i];
-        Fb[m * mstride + i] = make_double2(gn.x + gs.x, gn.y + gs.y);
-        Fb[m * mstride + a.JH + i] = make_double2(gn.x - gs.x, gn.y - gs.y);
-      }
-    }
-    __syncthreads();  // the buffer is refilled by the prefetch of the next iteration
+    fwd_tile<A, B, NT>(a, v, cur, stw, stwI, col, h0, j, valid);
+    __syncthreads();  // the output runs are read; the next tile reuses the buffer
   }
-  cp_async_wait<0>();
 }
 
 // Inverse transform, persistent over tiles; the Fourier runs of tile
@@ -523,36 +496,25 @@ int persistent_blocks(K kern, size_t smem, const sht_plan *p, long long ntiles)
 }
 
 template <int A, int B>
-int run_fft(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t s)
+int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
 {
   using S = FftShape<A, B, kFftThreads>;
-  int bufe = S::buf_elems(p->N);
-  FftArgs a = args;
-  if (!inverse && a.mul) {
-    // room for the factor's tile beside the data tile, where that costs no
-    // resident block (otherwise the first pass reads the factor through the
-    // read-only cache)
-    const int two = (2 * S::JT * S::NCp + 7) & ~7;
-    const int want = bufe > two ? bufe : two;
-    auto bytes = [](int e) { return sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)e); };
-    auto per_sm = [](size_t b) { return (int)((228 * 1024) / (b + 1024)); };
-    a.mul_staged = bytes(want) <= 227 * 1024 && per_sm(bytes(want)) >= per_sm(bytes(bufe));
-    if (a.mul_staged) bufe = want;
-  }
-  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + 2 * (size_t)bufe);
-  const long long ntiles = (long long)args.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
+  // inverse: two buffers (staged Fourier runs of the next tile beside the
+  // current one); forward: one buffer
+  const int bufe = S::buf_elems(p->N);
+  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + (inverse ? 2 : 1) * (size_t)bufe);
+  const long long ntiles = (long long)a.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
   if (ntiles <= 0) return SHT_OK;
   if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
   cudaError_t e = cudaSuccess;
-  auto go = [&](auto kern) {
+  auto go = [&](auto kern, auto... extra) {
     if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return;
-    kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(a, bufe);
+    kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(a, extra...);
   };
-  if (inverse) go(k_fft_inv<A, B, kFftThreads>);
-  else if (!a.mul) go(k_fft_fwd<A, B, kFftThreads, 0>);
-  else if (a.mul_staged) go(k_fft_fwd<A, B, kFftThreads, 1>);
-  else go(k_fft_fwd<A, B, kFftThreads, 2>);
+  if (inverse) go(k_fft_inv<A, B, kFftThreads>, bufe);
+  else if (a.mul) go(k_fft_fwd<A, B, kFftThreads, 1>);
+  else go(k_fft_fwd<A, B, kFftThreads, 0>);
   if (e != cudaSuccess) return cuda_fail(e, "fft smem attribute");
   count_launch();
   e = cudaGetLastError();
