@@ -37,7 +37,8 @@ def nvcc() -> str:
 
 
 def _headers():
-    return glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(ROOT, "include", "*.h"))
+    return (glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+            + glob.glob(os.path.join(ROOT, "include", "*.h")))
 
 
 def _stale(target: str, deps) -> bool:

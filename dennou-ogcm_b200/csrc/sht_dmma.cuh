@@ -22,9 +22,11 @@ __device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0
 // d (8x8 FP64 tile, two values per lane) += a (8x4, one per lane) * b (4x8, one per lane)
 __device__ __forceinline__ void mma884(double (&d)[2], double a, double b)
 {
-  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
-               : "+d"(d[0]), "+d"(d[1])
-               : "d"(a), "d"(b));
+  // no side effects beyond d: left non-volatile so that the compiler may
+  // schedule fragment loads across the products
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+      : "+d"(d[0]), "+d"(d[1])
+      : "d"(a), "d"(b));
 }
 
 }  // namespace dmma

@@ -50,7 +50,7 @@ __host__ __device__ inline Geo make_geo(int N, int J)
   g.CS = round_mod(2 * J, 8, 16);
   g.AS = round_mod(2 * kCT, 2, 8);
   g.prow_cap = N + 4;
-  g.arow_cap = (N + 2 + 8 + 7) & ~7;  // rows of the larger band plus a zeroed tail (a k-step reads <= 5 past it)
+  g.arow_cap = (N + 2 + 8 + 7) & ~7;  // rows of the larger band plus a zeroed tail (a k-step reads up to 7 rows past it)
   return g;
 }
 
@@ -268,17 +268,20 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
 #pragma unroll
         for (int nt = 0; nt < 4; ++nt) acc[p][nt][0] = acc[p][nt][1] = 0.0;
       const int jcol = 8 * jt + (lane >> 2);
+      // both parities in one loop (8 independent product chains per warp):
+      // the odd rows run to the even count, their coefficient rows past R are
+      // the zeroed tail of the panel
+      const int kp = (R + 1) / 2;
+      for (int t0 = 0; t0 < kp; t0 += 4) {
+        const int r = 2 * (t0 + (lane & 3));
+        const double av0 = Pm[min(r, R - 1) * g.PS + jcol], av1 = Pm[min(r + 1, R - 1) * g.PS + jcol];
+        const double *brow = A + r * g.AS + (lane >> 2);
 #pragma unroll
-      for (int p = 0; p < 2; ++p) {
-        const int kp = (R - p + 1) / 2;  // rows of this parity
-        for (int t0 = 0; t0 < kp; t0 += 4) {
-          const int r = p + 2 * (t0 + (lane & 3));
-          const double av = Pm[min(r, R - 1) * g.PS + jcol];
-          const double *brow = A + r * g.AS + (lane >> 2);
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if (q < nnt) mma884(acc[p][q], av, brow[8 * (grp * nnt + q)]);
-        }
+        for (int q = 0; q < 4; ++q)
+          if (q < nnt) {
+            mma884(acc[0][q], av0, brow[8 * (grp * nnt + q)]);
+            mma884(acc[1][q], av1, brow[g.AS + 8 * (grp * nnt + q)]);
+          }
       }
       const int jh = 8 * jt + (lane >> 2);
 #pragma unroll
