@@ -65,6 +65,17 @@ __device__ __forceinline__ double2 csub(double2 x, double2 y) { return make_doub
 __device__ __forceinline__ double2 cscale(double2 x, double s) { return make_double2(x.x * s, x.y * s); }
 __device__ __forceinline__ double2 times_im(double2 x, int m) { return make_double2(-m * x.y, m * x.x); }
 
+// Which internal rows a pack operator reads: degree offset dn in -1..1 of
+// column set `set` (0: the first input's columns, 1: the second's).
+template <int OP>
+__host__ __device__ constexpr bool pack_needs(int dn, int set)
+{
+  return OP == PACK_PLAIN || OP == PACK_DIVLAMBDA ? (dn == 0 && set == 0)
+       : OP == PACK_DIVMU                         ? (dn != 0 && set == 0)
+       : OP == PACK_ALPHA                         ? (set == 0 ? dn == 0 : dn != 0)
+                                                  : true;  // VORDIV
+}
+
 template <int OP>
 __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
 {
@@ -75,33 +86,47 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int b = b0 + lane;
   constexpr int NOUT = (OP == PACK_VORDIV) ? 2 : 1;
+  constexpr int NI = kMC / 8;  // orders per warp
+  // every load of the thread is issued before any is used: out-of-range
+  // entries read element 0 and are replaced by zero
+  double2 c[NI][3][2];
 #pragma unroll
-  for (int mi = warp; mi < kMC; mi += 8) {
-    const int m = m0 + mi;
+  for (int i = 0; i < NI; ++i) {
+    const int m = m0 + warp + 8 * i;
+    const bool ok = m <= n && m < a.M && b < a.nb;
+    const long long base = ok ? (long long)(__ldg(a.rowoff + m) + (n - m)) * a.ncolS + b : 0;
+#pragma unroll
+    for (int dn = -1; dn <= 1; ++dn)
+#pragma unroll
+      for (int set = 0; set < 2; ++set) {
+        c[i][dn + 1][set] = make_double2(0.0, 0.0);
+        if (!pack_needs<OP>(dn, set)) continue;
+        const bool okk = ok && n + dn >= m && n + dn <= a.N + 1;
+        const double2 x = a.S[okk ? base + (long long)dn * a.ncolS + set * a.nb : 0];
+        if (okk) c[i][dn + 1][set] = x;
+      }
+  }
+#pragma unroll
+  for (int i = 0; i < NI; ++i) {
+    const int mi = warp + 8 * i, m = m0 + mi;
     double2 v0 = make_double2(0.0, 0.0), v1 = make_double2(0.0, 0.0);
     if (m <= n && m < a.M && b < a.nb) {
-      const long long base = (long long)(__ldg(a.rowoff + m) + (n - m)) * a.ncolS;
-      auto ld = [&](int dn, int set) -> double2 {
-        const int nn = n + dn;
-        if (nn < m || nn > a.N + 1) return make_double2(0.0, 0.0);
-        return a.S[base + (long long)dn * a.ncolS + set * a.nb + b];
-      };
       auto D = [&](int set) -> double2 {  // -( (n+1) eps_n c_{n-1} - n eps_{n+1} c_{n+1} )
         const double e0 = (n + 1) * eps_at(a, m, n), e1 = n * eps_at(a, m, n + 1);
-        const double2 cm = ld(-1, set), cp = ld(1, set);
+        const double2 cm = c[i][0][set], cp = c[i][2][set];
         return make_double2(e1 * cp.x - e0 * cm.x, e1 * cp.y - e0 * cm.y);
       };
       if (OP == PACK_PLAIN) {
-        v0 = ld(0, 0);
+        v0 = c[i][1][0];
       } else if (OP == PACK_DIVLAMBDA) {
-        v0 = times_im(ld(0, 0), m);
+        v0 = times_im(c[i][1][0], m);
       } else if (OP == PACK_DIVMU) {
         v0 = D(0);
       } else if (OP == PACK_ALPHA) {
-        v0 = cscale(cadd(times_im(ld(0, 0), m), D(1)), 1.0 / a.radius);
+        v0 = cscale(cadd(times_im(c[i][1][0], m), D(1)), 1.0 / a.radius);
       } else {  // PACK_VORDIV: set 0 = U cos, set 1 = V cos
-        v0 = cscale(csub(times_im(ld(0, 1), m), D(0)), 1.0 / a.radius);
-        v1 = cscale(cadd(times_im(ld(0, 0), m), D(1)), 1.0 / a.radius);
+        v0 = cscale(csub(times_im(c[i][1][1], m), D(0)), 1.0 / a.radius);
+        v1 = cscale(cadd(times_im(c[i][1][0], m), D(1)), 1.0 / a.radius);
       }
     }
     const double s = (m == 0) ? 1.0 : kSqrt2;
