@@ -9,7 +9,8 @@
 // current one is contracted on the FP64 tensor path (mma.sync.m8n8k4.f64).
 // Shared-memory row strides are chosen so that every 16-lane phase of a
 // fragment load touches 16 distinct double-word bank pairs:
-//   P rows (stride-2 rows of one parity):  PS = 2 (mod 8) doubles
+//   P rows (stride-2 rows of one parity):  PS = 2 (mod 8) doubles (synthesis,
+//     8-byte fragment loads), 4 (mod 8) (analysis, 16-byte fragment loads)
 //   data rows (columns of one panel):      CS = 8 (mod 16) doubles
 //   coefficient rows (stride-2 rows):      AS = 2 (mod 8) doubles
 // Used when a pair's P rows and two data panels fit in shared memory (T85 and
@@ -42,11 +43,11 @@ __host__ __device__ inline int round_mod(int x, int r, int mod)
   return x;
 }
 
-__host__ __device__ inline Geo make_geo(int N, int J)
+__host__ __device__ inline Geo make_geo(int N, int J, bool analysis)
 {
   Geo g;
   const int JH = J / 2;
-  g.PS = round_mod(JH, 2, 8);
+  g.PS = round_mod(JH, analysis ? 4 : 2, 8);
   g.CS = round_mod(2 * J, 8, 16);
   g.AS = round_mod(2 * kCT, 2, 8);
   g.prow_cap = N + 4;
@@ -111,7 +112,7 @@ template <int JH>
 __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
 {
   extern __shared__ __align__(16) double sm[];
-  const Geo g = make_geo(a.N, 2 * JH);
+  const Geo g = make_geo(a.N, 2 * JH, true);
   double *Pbuf = sm;
   double *const G0 = sm + g.prow_cap * g.PS, *const G1 = G0 + 2 * kCT * g.CS;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -159,22 +160,38 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
       const double *G = Gcur + mi * kCT * g.CS + (par ? 2 * JH : 0);
       const int r0 = par + 2 * (16 * gi + (lane >> 2));
       const int r1 = r0 + 16;
-      const double *pa0 = Pm + min(r0, R - 1) * g.PS + (lane & 3);
-      const double *pa1 = Pm + min(r1, R - 1) * g.PS + (lane & 3);
-      const double *gb = G + (lane >> 3) * g.CS + ((lane >> 2) & 1) + 2 * (lane & 3);
-      double acc[2][4][2];
+      // K order within each pair of k-steps: lane q = lane & 3 takes latitude
+      // 8j + 2q in the first and 8j + 2q + 1 in the second, so one 16-byte
+      // load gives a lane both A values.  The columns form four 8-column
+      // tiles (colrow half h, real / imaginary part): one 16-byte load gives a
+      // lane the B values (re, im) of its colrow for two tiles.
+      const int q = lane & 3;
+      const double *pa0 = Pm + min(r0, R - 1) * g.PS + 2 * q;
+      const double *pa1 = Pm + min(r1, R - 1) * g.PS + 2 * q;
+      const double *gb = G + (lane >> 2) * g.CS + 4 * q;
+      double acc[2][2][2][2];  // [row tile][colrow half][re/im][2 columns]
 #pragma unroll
       for (int t = 0; t < 2; ++t)
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) acc[t][nt][0] = acc[t][nt][1] = 0.0;
+        for (int h = 0; h < 2; ++h)
 #pragma unroll
-      for (int kb = 0; kb < JH; kb += 4) {
-        const double a0 = pa0[kb], a1 = pa1[kb];
+          for (int pt = 0; pt < 2; ++pt) acc[t][h][pt][0] = acc[t][h][pt][1] = 0.0;
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          const double b = gb[4 * nt * g.CS + 2 * kb];
-          mma884(acc[0][nt], a0, b);
-          mma884(acc[1][nt], a1, b);
+      for (int kb = 0; kb < JH; kb += 8) {
+        const double2 a0 = *reinterpret_cast<const double2 *>(pa0 + kb);
+        const double2 a1 = *reinterpret_cast<const double2 *>(pa1 + kb);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+          const double2 be = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb);      // latitude 8j + 2q
+          const double2 bo = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb + 2);  // latitude 8j + 2q + 1
+          mma884(acc[0][h][0], a0.x, be.x);
+          mma884(acc[0][h][1], a0.x, be.y);
+          mma884(acc[1][h][0], a1.x, be.x);
+          mma884(acc[1][h][1], a1.x, be.y);
+          mma884(acc[0][h][0], a0.y, bo.x);
+          mma884(acc[0][h][1], a0.y, bo.y);
+          mma884(acc[1][h][0], a1.y, bo.x);
+          mma884(acc[1][h][1], a1.y, bo.y);
         }
       }
       const long long rowbase = a.rowoff[m];
@@ -183,10 +200,12 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
         const int r = par + 2 * (16 * gi + 8 * t + (lane >> 2));
         if (r >= R) continue;
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) {
-          const int c = col0 + 4 * nt + (lane & 3);
-          if (c < a.ncol) a.S[(rowbase + r) * a.ncol + c] = make_double2(acc[t][nt][0], acc[t][nt][1]);
-        }
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int c = col0 + 8 * h + 2 * q + e;
+            if (c < a.ncol) a.S[(rowbase + r) * a.ncol + c] = make_double2(acc[t][h][0][e], acc[t][h][1][e]);
+          }
       }
     }
     __syncthreads();
@@ -219,7 +238,7 @@ template <int JH>
 __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
 {
   extern __shared__ __align__(16) double sm[];
-  const Geo g = make_geo(a.N, 2 * JH);
+  const Geo g = make_geo(a.N, 2 * JH, false);
   double *Pbuf = sm;
   const int abuf = 2 * g.arow_cap * g.AS;
   double *const A0 = sm + g.prow_cap * g.PS, *const A1 = A0 + abuf;
@@ -301,12 +320,12 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
 
 size_t fwd_smem(int N, int J)
 {
-  const Geo g = make_geo(N, J);
+  const Geo g = make_geo(N, J, true);
   return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * 2 * kCT * (size_t)g.CS);
 }
 size_t inv_smem(int N, int J)
 {
-  const Geo g = make_geo(N, J);
+  const Geo g = make_geo(N, J, false);
   return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * 2 * (size_t)g.arow_cap * g.AS);
 }
 

@@ -210,9 +210,16 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
   __syncthreads();
   const int b = b0 + lane;
   if (b >= a.nb) return;
-  for (int mi = warp; mi < kMC; mi += 8) {
-    const int m = m0 + mi;
-    if (m > n || m > a.N || m >= a.M) continue;
+  int rows[kMC / 8];  // row offsets of this warp's orders, loaded before the loop
+#pragma unroll
+  for (int i = 0; i < kMC / 8; ++i) {
+    const int m = m0 + warp + 8 * i;
+    rows[i] = (m <= n && m <= a.N && m < a.M) ? __ldg(a.rowoff + m) + (n - m) : -1;
+  }
+#pragma unroll
+  for (int i = 0; i < kMC / 8; ++i) {
+    const int mi = warp + 8 * i, m = m0 + mi;
+    if (rows[i] < 0) continue;
     const double s = (m == 0) ? 1.0 : kRSqrt2;
     auto coef = [&](int in, int dn) -> double2 {
       const int run = in * 6 + (dn + 1) * 2;
@@ -249,7 +256,7 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
       v0 = csub(times_im(chi, m), R(0, a2));
       v1 = cadd(times_im(psi, m), R(1, a2));
     }
-    const long long row = (long long)(__ldg(a.rowoff + m) + (n - m));
+    const long long row = rows[i];
     a.So[row * a.ncolS + b] = v0;
     if (OP == UNPACK_VORDIV2UV || OP == UNPACK_HGRAD) a.So[row * a.ncolS + a.nb + b] = v1;
   }
