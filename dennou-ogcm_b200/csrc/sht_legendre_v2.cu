@@ -291,26 +291,57 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
       // the odd rows run to the even count, their coefficient rows past R are
       // the zeroed tail of the panel
       const int kp = (R + 1) / 2;
-      for (int t0 = 0; t0 < kp; t0 += 4) {
-        const int r = 2 * (t0 + (lane & 3));
-        const double av0 = Pm[min(r, R - 1) * g.PS + jcol], av1 = Pm[min(r + 1, R - 1) * g.PS + jcol];
-        const double *brow = A + r * g.AS + (lane >> 2);
+      if constexpr (nnt % 2 == 0) {
+        // columns as (real part, imaginary part) tile pairs of 8 complex
+        // columns: one 16-byte load gives a lane its B values for both tiles
+        const int cb = 4 * grp * nnt;  // first complex column of this warp
+        for (int t0 = 0; t0 < kp; t0 += 4) {
+          const int r = 2 * (t0 + (lane & 3));
+          const double av0 = Pm[min(r, R - 1) * g.PS + jcol], av1 = Pm[min(r + 1, R - 1) * g.PS + jcol];
+          const double *brow = A + r * g.AS + 2 * (cb + (lane >> 2));
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          if (q < nnt) {
-            mma884(acc[0][q], av0, brow[8 * (grp * nnt + q)]);
-            mma884(acc[1][q], av1, brow[g.AS + 8 * (grp * nnt + q)]);
+          for (int u2 = 0; u2 < nnt / 2; ++u2) {
+            const double2 b0 = *reinterpret_cast<const double2 *>(brow + 16 * u2);
+            const double2 b1 = *reinterpret_cast<const double2 *>(brow + g.AS + 16 * u2);
+            mma884(acc[0][2 * u2], av0, b0.x);
+            mma884(acc[0][2 * u2 + 1], av0, b0.y);
+            mma884(acc[1][2 * u2], av1, b1.x);
+            mma884(acc[1][2 * u2 + 1], av1, b1.y);
           }
-      }
-      const int jh = 8 * jt + (lane >> 2);
+        }
+        const int jh = 8 * jt + (lane >> 2);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        if (q >= nnt) continue;
-        const int c = col0 + 4 * (grp * nnt + q) + (lane & 3);
-        if (c >= a.ncol) continue;
-        double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
-        Fc[jh] = make_double2(acc[0][q][0], acc[0][q][1]);       // even degrees
-        Fc[JH + jh] = make_double2(acc[1][q][0], acc[1][q][1]);  // odd degrees
+        for (int u2 = 0; u2 < nnt / 2; ++u2)
+#pragma unroll
+          for (int e = 0; e < 2; ++e) {
+            const int c = col0 + cb + 8 * u2 + 2 * (lane & 3) + e;
+            if (c >= a.ncol) continue;
+            double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
+            Fc[jh] = make_double2(acc[0][2 * u2][e], acc[0][2 * u2 + 1][e]);       // even degrees
+            Fc[JH + jh] = make_double2(acc[1][2 * u2][e], acc[1][2 * u2 + 1][e]);  // odd degrees
+          }
+      } else {
+        for (int t0 = 0; t0 < kp; t0 += 4) {
+          const int r = 2 * (t0 + (lane & 3));
+          const double av0 = Pm[min(r, R - 1) * g.PS + jcol], av1 = Pm[min(r + 1, R - 1) * g.PS + jcol];
+          const double *brow = A + r * g.AS + (lane >> 2);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            if (q < nnt) {
+              mma884(acc[0][q], av0, brow[8 * (grp * nnt + q)]);
+              mma884(acc[1][q], av1, brow[g.AS + 8 * (grp * nnt + q)]);
+            }
+        }
+        const int jh = 8 * jt + (lane >> 2);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          if (q >= nnt) continue;
+          const int c = col0 + 4 * (grp * nnt + q) + (lane & 3);
+          if (c >= a.ncol) continue;
+          double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
+          Fc[jh] = make_double2(acc[0][q][0], acc[0][q][1]);       // even degrees
+          Fc[JH + jh] = make_double2(acc[1][q][0], acc[1][q][1]);  // odd degrees
+        }
       }
     }
     __syncthreads();
