@@ -274,7 +274,10 @@ def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
       followed by w_AlphaOptr_xy (the tracer flux divergence of the thickness
       equation, Q = H cos(phi) T);
     - Redi/GM gradients: xy_HGrad_xy(T) against w_xy then xy_GradLon_w and
-      xy_GradLat_w."""
+      xy_GradLat_w;
+    - batched callers: the transform parts of the tracer and momentum
+      tendency loops over 60 levels in one call per operator, against the
+      same operators called level by level."""
     nb = args.nb or 480
     g = torch.Generator(device=dev).manual_seed(20261203)
     shape = (nb, sht.jm, sht.im)
@@ -319,6 +322,22 @@ def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
         out[name] = {"fused_ms": tf, "unfused_ms": tu, "speedup": tu / tf, "relerr_vs_unfused": err}
     # the same analysis without the products: what the product epilogue adds
     out["alphaoptr_prod"]["alphaoptr_without_products_ms"] = timeit(lambda: sht.w_AlphaOptr_xy(A, B))
+
+    # the per-level loops of HBEBaroc_HTRCRHS and HBEBaroc_MOMRHS_VorDivForm
+    # (one field, 60 levels) as batched calls against the same calls issued
+    # level by level from this host, as the reference's do-k loops do
+    C = importlib.import_module("dennou-ogcm_b200.callers")
+    K = 60
+    lvl = (A[:K], B[:K], T[:K], Q[:K])
+    filt = torch.ones(sht.lm, dtype=torch.float64, device=dev)
+    hp = torch.zeros_like(A[:K])
+    cases = {"htrc_rhs": (C.htrc_rhs, (*lvl, filt, hp)), "momrhs_vordiv": (C.momrhs_vordiv, lvl[:3])}
+    calls = {}
+    for name, (fn, xs) in cases.items():
+        tb = timeit(lambda: fn(sht, *xs))
+        tl = timeit(lambda: C.per_level(fn, sht, *xs))
+        calls[name] = {"levels": K, "batched_ms": tb, "per_level_ms": tl, "speedup": tl / tb}
+    out["batched_callers"] = calls
     return out
 
 

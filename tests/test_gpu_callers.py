@@ -1,0 +1,77 @@
+"""Batched callers (dennou-ogcm_b200/callers.py): the spectral parts of the
+per-level loops of HBEBaroc_HTRCRHS (HBEBaroc_hspm_vfvm_mod.f90:160-172) and
+HBEBaroc_MOMRHS_VorDivForm (:430-441) as calls over all levels.
+
+Oracle: the loops' formulas composed from the CPU restatement's operators as
+the reference writes them (w_AlphaOptr_xy(B, -A) for the divergence
+tendency, not the calc_UVCosLat2VorDiv identity the batched form uses).
+The level-by-level form through the library must agree with the batched one.
+Tolerance 1e-11 per field, as for every FP64 operator.
+"""
+import importlib
+
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from conftest import pkg, relerr, workloads
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-11
+A = 6.371e6
+
+
+def callers():
+    return importlib.import_module("dennou-ogcm_b200.callers")
+
+
+@pytest.fixture(scope="module")
+def t42():
+    I, J, N = workloads().GRIDS["T42"]
+    sp = pkg().SpmlUtil(I, J, 12, N, None, A)
+    yield sp, O.OraclePlan(I, J, N, A)
+    sp.final()
+
+
+def _grids(K, J, I, n, seed):
+    rng = np.random.default_rng(seed)
+    return [rng.standard_normal((K, J, I)) for _ in range(n)]
+
+
+def test_htrc_rhs_batched_vs_oracle_and_per_level(t42):
+    sp, ora = t42
+    C = callers()
+    K = 12
+    u, v, tmp, vflx, hphys = _grids(K, sp.jm, sp.im, 5, seed=1)
+    n = np.floor(np.sqrt(np.arange(sp.lm)))
+    filt = np.exp(-((n / sp.nm) ** 8))  # an AdvFilter-like spectral taper
+    w = ora.wa_xya(vflx) - ora.wa_alphaoptr_xya(u * tmp, v * tmp)
+    ref = ora.xya_wa(w * filt[None, :]) + hphys
+    d = [torch.from_numpy(x).cuda() for x in (u, v, tmp, vflx)]
+    f, hp = torch.from_numpy(filt).cuda(), torch.from_numpy(hphys).cuda()
+    out = C.htrc_rhs(sp, *d, f, hp)
+    lvl = C.per_level(C.htrc_rhs, sp, *d, f, hp)
+    torch.cuda.synchronize()
+    assert relerr(out.cpu().numpy(), ref) < TOL
+    assert relerr(lvl.cpu().numpy(), out.cpu().numpy()) < 1e-13
+
+
+def test_momrhs_vordiv_batched_vs_oracle_and_per_level(t42):
+    sp, ora = t42
+    C = callers()
+    K = 12
+    a, b, c = _grids(K, sp.jm, sp.im, 3, seed=2)
+    cs = np.cos(sp.y_Lat)[None, :, None]
+    a, b = a * cs, b * cs  # xy_A and xy_B carry cos(phi)
+    vor_rhs = -ora.wa_alphaoptr_xya(a, b)
+    div_rhs = ora.wa_alphaoptr_xya(b, -a) - ora.wa_lapla_wa(ora.wa_xya(c))
+    ur, vr = ora.vordiv2uv(vor_rhs, div_rhs)
+    d = [torch.from_numpy(x).cuda() for x in (a, b, c)]
+    u, v = C.momrhs_vordiv(sp, *d)
+    ul, vl = C.per_level(C.momrhs_vordiv, sp, *d)
+    torch.cuda.synchronize()
+    assert relerr(u.cpu().numpy(), ur) < TOL and relerr(v.cpu().numpy(), vr) < TOL
+    assert relerr(ul.cpu().numpy(), u.cpu().numpy()) < 1e-13
+    assert relerr(vl.cpu().numpy(), v.cpu().numpy()) < 1e-13
