@@ -183,6 +183,7 @@ enum Op : int {
   OP_W_ALPHA_PROD,  // w_AlphaOptr_xy(A Q, B Q): third input Q
   OP_HGRAD,         // xy_GradLon_w and xy_GradLat_w of one spectrum
   OP_HGRAD_G,       // the same of w_xy(grid)
+  OP_FLUXDIV_G,     // xy_w(w_AlphaOptr_xy(A, B)), grid to grid
 };
 
 struct OpShape {
@@ -199,6 +200,7 @@ OpShape shape_of(int op)
   case OP_W_ALPHA_PROD: return {3, 1, true, false};
   case OP_HGRAD: return {1, 2, false, true};
   case OP_HGRAD_G: return {1, 2, true, true};
+  case OP_FLUXDIV_G: return {2, 1, true, true};
   case OP_XY_ALPHA: return {2, 1, false, true};
   case OP_UV2VORDIV: return {2, 2, true, false};
   case OP_VORDIV2UV: return {2, 2, false, true};
@@ -223,6 +225,13 @@ int run_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, dou
     if (rc) return rc;
     if ((rc = run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, i0, nullptr, nb, ws.W, nullptr))) return rc;
     return run_synthesis(p, UNPACK_HGRAD, RS_INV_INVCOS, ws.W, nullptr, nb, o0, o1);
+  }
+  case OP_FLUXDIV_G: {
+    Workspace ws;
+    int rc = ensure_ws(p, 2 * nb, nb, &ws);
+    if (rc) return rc;
+    if ((rc = run_analysis(p, PACK_ALPHA, RS_FWD_INV1MMU2, i0, i1, nb, ws.W, nullptr))) return rc;
+    return run_synthesis(p, UNPACK_PLAIN, RS_INV_PLAIN, ws.W, nullptr, nb, o0, nullptr);
   }
   case OP_W_XY: return run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, i0, nullptr, nb, o0, nullptr);
   case OP_DIVLAMBDA: return run_analysis(p, PACK_DIVLAMBDA, RS_FWD_INV1MMU2, i0, nullptr, nb, o0, nullptr);
@@ -700,6 +709,10 @@ int sht_xya_hgrad_xya(sht_plan *p, const double *x, int nb, double *lon, double 
 { return api_host(p, OP_HGRAD_G, x, nullptr, nb, lon, lat); }
 int sht_xya_hgrad_xya_dev(sht_plan *p, const double *x, int nb, double *lon, double *lat)
 { return api_dev(p, OP_HGRAD_G, x, nullptr, nb, lon, lat); }
+int sht_xya_fluxdiv_xya(sht_plan *p, const double *a, const double *b, int nb, double *x)
+{ return api_host(p, OP_FLUXDIV_G, a, b, nb, x, nullptr); }
+int sht_xya_fluxdiv_xya_dev(sht_plan *p, const double *a, const double *b, int nb, double *x)
+{ return api_dev(p, OP_FLUXDIV_G, a, b, nb, x, nullptr); }
 int sht_uvcoslat2vordiv(sht_plan *p, const double *u, const double *v, int nb, double *vor, double *div)
 { return api_host(p, OP_UV2VORDIV, u, v, nb, vor, div); }
 int sht_uvcoslat2vordiv_dev(sht_plan *p, const double *u, const double *v, int nb, double *vor, double *div)

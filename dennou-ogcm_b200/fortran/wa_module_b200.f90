@@ -31,7 +31,7 @@ module wa_module_b200
   public :: b200_wa_AlphaOptr_xya, b200_xya_AlphaOptr_wa
   public :: b200_calc_UVCosLat2VorDiv, b200_calc_VorDiv2UV
   public :: b200_wa_Diffuse
-  public :: b200_wa_AlphaOptrProd_xya, b200_xya_HGrad_wa, b200_xya_HGrad_xya
+  public :: b200_wa_AlphaOptrProd_xya, b200_xya_HGrad_wa, b200_xya_HGrad_xya, b200_xya_FluxDiv_xya
 
   integer, parameter :: SHT_OK = 0
   character(*), parameter :: module_name = 'wa_module_b200'
@@ -181,6 +181,11 @@ module wa_module_b200
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: plan; real(c_double), intent(in) :: x(*)
       integer(c_int), value :: nb; real(c_double), intent(out) :: glon(*), glat(*)
+    end function
+    integer(c_int) function sht_xya_fluxdiv_xya(plan, a, b, nb, x) bind(C, name='sht_xya_fluxdiv_xya')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: a(*), b(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: x(*)
     end function
     integer(c_int) function sht_wa_diffuse(plan, w, nb, coef, dt, filt) bind(C, name='sht_wa_diffuse')
       import :: c_int, c_double, c_ptr
@@ -443,5 +448,14 @@ contains
     real(DP), intent(out) :: xya_GradLon(:,:,:), xya_GradLat(:,:,:)
     call check(sht_xya_hgrad_xya(plan, xya, int(size(xya, 3), c_int), xya_GradLon, xya_GradLat), 'xya_HGrad_xya')
   end subroutine b200_xya_HGrad_xya
+
+  !> xya_wa(wa_AlphaOptr_xya(A, B)) grid to grid: the Redi/GM flux divergence
+  !> (physics/lphys/LPhys_RediGM_hspm_vfvm_mod.f90:350-355)
+  function b200_xya_FluxDiv_xya(xya_A, xya_B)
+    real(DP), intent(in) :: xya_A(:,:,:), xya_B(:,:,:)
+    real(DP) :: b200_xya_FluxDiv_xya(0:im-1, jm, size(xya_A, 3))
+    call check(sht_xya_fluxdiv_xya(plan, xya_A, xya_B, int(size(xya_A, 3), c_int), b200_xya_FluxDiv_xya), &
+         'xya_FluxDiv_xya')
+  end function b200_xya_FluxDiv_xya
 
 end module wa_module_b200

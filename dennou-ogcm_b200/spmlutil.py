@@ -42,7 +42,7 @@ _G2S = ["sht_wa_xya", "sht_xya_wa", "sht_wa_divlambda_xya", "sht_wa_divmu_xya",
         "sht_xya_gradlambda_wa", "sht_xya_gradmu_wa", "sht_xya_gradlon_wa",
         "sht_xya_gradlat_wa", "sht_wa_lapla_wa", "sht_wa_laplainv_wa",
         "sht_avrlonlat_xya", "sht_intlonlat_xya", "sht_ya_avrlon_xya", "sht_ya_intlon_xya"]
-_TWO_IN = ["sht_wa_alphaoptr_xya", "sht_xya_alphaoptr_wa"]
+_TWO_IN = ["sht_wa_alphaoptr_xya", "sht_xya_alphaoptr_wa", "sht_xya_fluxdiv_xya"]
 _TWO_IO = ["sht_uvcoslat2vordiv", "sht_vordiv2uv"]
 _ONE_IN_TWO_OUT = ["sht_xya_hgrad_wa", "sht_xya_hgrad_xya"]
 
@@ -364,7 +364,12 @@ class SpmlUtil:
         gradients before the 1/radius factor (LPhys_RediGM_hspm_vfvm_mod.f90:432-440)."""
         return self._run("sht_xya_hgrad_xya", [xy], "grid", nout=2)
 
+    def xy_FluxDiv_xy(self, xy_A, xy_B):
+        """xy_w(w_AlphaOptr_xy(A, B)), grid to grid (LPhys_RediGM_hspm_vfvm_mod.f90:350-355)."""
+        return self._run("sht_xya_fluxdiv_xya", [xy_A, xy_B], "grid")
+
     wa_AlphaOptrProd_xya = w_AlphaOptrProd_xy
+    xya_FluxDiv_xya = xy_FluxDiv_xy
     xya_HGrad_wa = xy_HGrad_w
     xya_HGrad_xya = xy_HGrad_xy
 

@@ -183,6 +183,14 @@ SHT_API int sht_xya_hgrad_wa(sht_plan *plan, const double *wa, int nb, double *x
 SHT_API int sht_xya_hgrad_xya(sht_plan *plan, const double *xya, int nb, double *xya_lon,
                       double *xya_lat);
 
+/* xy_w(w_AlphaOptr_xy(A, B)) grid to grid: the divergence of the Redi/GM
+ * tracer fluxes added to the tendency (physics/lphys/
+ * LPhys_RediGM_hspm_vfvm_mod.f90:350-355, A and B the flux components times
+ * cos(phi)).  One analysis of 2 nb columns into a device temp, then one
+ * synthesis; no spectral array on the caller's side. */
+SHT_API int sht_xya_fluxdiv_xya(sht_plan *plan, const double *xya_a, const double *xya_b, int nb,
+                        double *xya);
+
 /* calc_UVCosLat2VorDiv: Vor = H(V cos, -U cos), Div = H(U cos, V cos)
  * (SpmlUtil_mod.f90:299-314, 342-368). Inputs are U cos phi and V cos phi. */
 SHT_API int sht_uvcoslat2vordiv(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
@@ -233,6 +241,8 @@ SHT_API int sht_xya_hgrad_wa_dev(sht_plan *plan, const double *wa, int nb, doubl
                          double *xya_lat);
 SHT_API int sht_xya_hgrad_xya_dev(sht_plan *plan, const double *xya, int nb, double *xya_lon,
                           double *xya_lat);
+SHT_API int sht_xya_fluxdiv_xya_dev(sht_plan *plan, const double *xya_a, const double *xya_b, int nb,
+                            double *xya);
 SHT_API int sht_uvcoslat2vordiv_dev(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
                             int nb, double *wa_vor, double *wa_div);
 SHT_API int sht_vordiv2uv_dev(sht_plan *plan, const double *wa_vor, const double *wa_div,

@@ -70,6 +70,7 @@ def test_fused_clients_check_arguments_on_the_host():
     assert lib.sht_wa_alphaoptr_prod_xya_dev(None, buf, buf, buf, 1, buf) == 3
     assert lib.sht_xya_hgrad_wa(None, buf, 1, buf, buf) == 3
     assert lib.sht_xya_hgrad_xya_dev(None, buf, 1, buf, buf) == 3
+    assert lib.sht_xya_fluxdiv_xya(None, buf, buf, 1, buf) == 3
 
 
 def test_init_without_device_reports_no_device(cuda_available):

@@ -6,7 +6,9 @@ horizontal-gradient composites.
   the products formed inside the longitude transform;
 - xy_HGrad_w(w) = (xy_GradLon_w(w), xy_GradLat_w(w)) in one synthesis;
 - xy_HGrad_xy(T) = the same of w_xy(T), the Redi/GM tracer gradients of
-  physics/lphys/LPhys_RediGM_hspm_vfvm_mod.f90:432-440 (before 1/radius).
+  physics/lphys/LPhys_RediGM_hspm_vfvm_mod.f90:432-440 (before 1/radius);
+- xy_FluxDiv_xy(A, B) = xy_w(w_AlphaOptr_xy(A, B)), the Redi/GM flux
+  divergence of the same file, :350-355.
 
 Oracle: the CPU restatement, with the products formed in numpy and the
 gradients composed from its single operators.  Tolerance 1e-11 per field, as
@@ -165,5 +167,35 @@ def test_hgrad_zonal():
         w = np.zeros((4, (z.nm + 1) ** 2))
         w[:, n * (n + 1)] = z.w_xy(x)
         assert relerr(z.xy_HGrad_w(z.w_xy(x))[1], full.xya_gradlat_wa(w)[:, :, :1]) < TOL
+    finally:
+        z.final()
+
+
+@pytest.mark.parametrize("grid", GRIDS[:3])
+def test_fluxdiv_grid_to_grid_vs_oracle(grid, plans):
+    I, J, N = grid
+    gpu, ora = plans(I, J, N, A)
+    a, b, _ = _grids(4, J, I, seed=N + 5)
+    cs = np.cos(gpu.y_Lat)[None, :, None]
+    a, b = a * cs, b * cs
+    ref = ora.xya_wa(ora.wa_alphaoptr_xya(a, b))
+    assert relerr(gpu.xy_FluxDiv_xy(a, b), ref) < TOL
+    out = gpu.xy_FluxDiv_xy(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda())
+    torch.cuda.synchronize()
+    assert relerr(out.cpu().numpy(), ref) < TOL
+
+
+def test_fluxdiv_pipelined_and_zonal(plans):
+    gpu, ora = plans(128, 64, 42, A)
+    a, b, _ = _grids(100, 64, 128, seed=31)  # host arrays: a pipeline of two chunks
+    assert relerr(gpu.xy_FluxDiv_xy(a, b), ora.xya_wa(ora.wa_alphaoptr_xya(a, b))) < TOL
+    z = pkg().SpmlUtil(1, 64, 1, -1, None, A)
+    try:
+        za, zb, _ = _grids(5, 64, 1, seed=32)
+        io = _io(z.nm)
+        full = O.OraclePlan(io, 64, z.nm, A)
+        rep = lambda x: np.repeat(x, io, axis=2)
+        ref = full.xya_wa(full.wa_alphaoptr_xya(rep(za), rep(zb)))[:, :, :1]
+        assert relerr(z.xy_FluxDiv_xy(za, zb), ref) < TOL
     finally:
         z.final()
