@@ -1,10 +1,11 @@
 """Batched forms of dogcm's per-level transform loops.
 
 dogcm calls the SpmlUtil operators one level at a time inside `do k` loops
-(dynamics/hspm_vfvm/HBEBaroc_hspm_vfvm_mod.f90:160-172 and :388-441).  On the
+(dynamics/hspm_vfvm/HBEBaroc_hspm_vfvm_mod.f90:160-172 and :388-441,
+dynamics/hspm_vfvm/HBEDiagnose_hspm_vfvm_mod.f90:276-284).  On the
 GPU a per-level call is a handful of small kernel launches and is bound by
 launch latency; the same loop as one call over all levels runs the kernels
-once over K columns.  These functions are the spectral parts of the two loops
+once over K columns.  These functions are the spectral parts of those loops
 written that way, on a SpmlUtil plan and CUDA float64 tensors of shape
 (K, jm, im) (grids) or (K, lm) (spectra).  The grid-space terms the loops
 build from the model state (the vertical flux divergence, the Coriolis and
@@ -45,6 +46,23 @@ def momrhs_vordiv(sp, a, b, c):
     analysis of both fields.  Four calls for all levels."""
     vor, div = sp.calc_UVCosLat2VorDiv(a, b)
     return sp.calc_VorDiv2UV(-div, vor - sp.w_Lapla_w(sp.w_xy(c)))
+
+
+def diagnose_vordiv(sp, u, v):
+    """Vorticity and divergence grids of HBEDiagnose_VorDiv
+    (HBEDiagnose_hspm_vfvm_mod.f90:276-284):
+
+        (w_Vor, w_Div) = calc_UVCosLat2VorDiv(U cos(phi), V cos(phi))
+        xyz_Vor = xy_w(w_Vor), xyz_Div = xy_w(w_Div)
+
+    One analysis of both fields and one synthesis of 2 K columns."""
+    import torch
+
+    cs = torch.cos(torch.as_tensor(sp.y_Lat, dtype=torch.float64, device=u.device))[None, :, None]
+    vor, div = sp.calc_UVCosLat2VorDiv(u * cs, v * cs)
+    K = u.shape[0]
+    g = sp.xy_w(torch.cat([vor, div]))
+    return g[:K], g[K:]
 
 
 def per_level(fn, sp, *arrays, **kw):

@@ -1,6 +1,7 @@
 """Batched callers (dennou-ogcm_b200/callers.py): the spectral parts of the
-per-level loops of HBEBaroc_HTRCRHS (HBEBaroc_hspm_vfvm_mod.f90:160-172) and
-HBEBaroc_MOMRHS_VorDivForm (:430-441) as calls over all levels.
+per-level loops of HBEBaroc_HTRCRHS (HBEBaroc_hspm_vfvm_mod.f90:160-172),
+HBEBaroc_MOMRHS_VorDivForm (:430-441) and HBEDiagnose_VorDiv
+(HBEDiagnose_hspm_vfvm_mod.f90:276-284) as calls over all levels.
 
 Oracle: the loops' formulas composed from the CPU restatement's operators as
 the reference writes them (w_AlphaOptr_xy(B, -A) for the divergence
@@ -75,3 +76,19 @@ def test_momrhs_vordiv_batched_vs_oracle_and_per_level(t42):
     assert relerr(u.cpu().numpy(), ur) < TOL and relerr(v.cpu().numpy(), vr) < TOL
     assert relerr(ul.cpu().numpy(), u.cpu().numpy()) < 1e-13
     assert relerr(vl.cpu().numpy(), v.cpu().numpy()) < 1e-13
+
+
+def test_diagnose_vordiv_batched_vs_oracle_and_per_level(t42):
+    sp, ora = t42
+    C = callers()
+    u, v = _grids(12, sp.jm, sp.im, 2, seed=3)
+    cs = np.cos(sp.y_Lat)[None, :, None]
+    wv, wd = ora.uvcoslat2vordiv(u * cs, v * cs)
+    rv, rd = ora.xya_wa(wv), ora.xya_wa(wd)
+    du, dv = torch.from_numpy(u).cuda(), torch.from_numpy(v).cuda()
+    gv, gd = C.diagnose_vordiv(sp, du, dv)
+    lv, ld = C.per_level(C.diagnose_vordiv, sp, du, dv)
+    torch.cuda.synchronize()
+    assert relerr(gv.cpu().numpy(), rv) < TOL and relerr(gd.cpu().numpy(), rd) < TOL
+    assert relerr(lv.cpu().numpy(), gv.cpu().numpy()) < 1e-13
+    assert relerr(ld.cpu().numpy(), gd.cpu().numpy()) < 1e-13
