@@ -29,7 +29,8 @@ namespace {
 
 constexpr int kW = 8;            // warps per block
 constexpr int kT = kW * 32;      // threads per block
-constexpr int kCT = 16;          // complex columns per item
+constexpr int kCT = 16;          // complex columns per item (synthesis)
+constexpr int kCTF = 8;          // complex columns per item (analysis: one panel, two blocks per SM)
 
 struct Geo {
   int PS, CS, AS;      // strides (doubles)
@@ -96,11 +97,11 @@ template <int JH>
 __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
 {
   constexpr int J = 2 * JH, RSTEP = kT / J;  // column rows covered per pass
-  const int nrow = (mb >= 0) ? 2 * kCT : kCT;
+  const int nrow = (mb >= 0) ? 2 * kCTF : kCTF;
   const int j = threadIdx.x % J;
 #pragma unroll 4
   for (int row = threadIdx.x / J; row < nrow; row += RSTEP) {
-    const int mi = row / kCT, b = row % kCT;
+    const int mi = row / kCTF, b = row % kCTF;
     const int m = mi ? mb : ma;
     const bool ok = col0 + b < a.ncol;
     const double2 *src = ok ? a.F + ((long long)m * a.ncol + col0 + b) * J + j : a.F;
@@ -109,40 +110,32 @@ __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma
 }
 
 template <int JH>
-__global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
+__global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
 {
+  // One data panel per block and two blocks per SM: each block's panel load
+  // overlaps the other block's products.
   extern __shared__ __align__(16) double sm[];
   const Geo g = make_geo(a.N, 2 * JH, true);
   double *Pbuf = sm;
-  double *const G0 = sm + g.prow_cap * g.PS, *const G1 = G0 + 2 * kCT * g.CS;
+  double *const G0 = sm + g.prow_cap * g.PS;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int it0 = blockIdx.x * a.per_cta;
   const int it1 = min(a.nitems, it0 + a.per_cta);
   if (it0 >= it1) return;
 
-  {
-    const int2 pr = a.pairs[it0 / a.ntiles];
-    load_F_panels<JH>(a, g, G0, pr.x, pr.y, (it0 % a.ntiles) * kCT);
-    cp_commit();
-  }
   int cur = -1;
   for (int it = it0; it < it1; ++it) {
-    const int bsel = (it - it0) & 1;
-    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCT;
+    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCTF;
     const int2 pr = a.pairs[pidx];
     if (pidx != cur) {
       load_pair_P<JH>(a, g, Pbuf, pr.x, pr.y);
       cur = pidx;
     }
+    load_F_panels<JH>(a, g, G0, pr.x, pr.y, col0);
     cp_commit();
-    if (it + 1 < it1) {
-      const int2 pn = a.pairs[(it + 1) / a.ntiles];
-      load_F_panels<JH>(a, g, bsel ? G0 : G1, pn.x, pn.y, ((it + 1) % a.ntiles) * kCT);
-    }
-    cp_commit();
-    cp_wait1();
+    cp_wait0();
     __syncthreads();
-    double *const Gcur = bsel ? G1 : G0;  // column rows: Gs at [0, JH), Ga at [JH, J)
+    double *const Gcur = G0;  // column rows: Gs at [0, JH), Ga at [JH, J)
 
     // jobs: (band, parity, 16-row group)
     const int Ra = a.N + 2 - pr.x, Rb = (pr.y >= 0) ? a.N + 2 - pr.y : 0;
@@ -157,7 +150,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
       else { mi = 1; par = 1; gi = job - gEa - gOa - gEb; }
       const int m = mi ? pr.y : pr.x, R = mi ? Rb : Ra;
       const double *Pm = Pbuf + (mi ? Ra : 0) * g.PS;
-      const double *G = Gcur + mi * kCT * g.CS + (par ? 2 * JH : 0);
+      const double *G = Gcur + mi * kCTF * g.CS + (par ? 2 * JH : 0);
       const int r0 = par + 2 * (16 * gi + (lane >> 2));
       const int r1 = r0 + 16;
       // K order within each pair of k-steps: lane q = lane & 3 takes latitude
@@ -169,11 +162,12 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
       const double *pa0 = Pm + min(r0, R - 1) * g.PS + 2 * q;
       const double *pa1 = Pm + min(r1, R - 1) * g.PS + 2 * q;
       const double *gb = G + (lane >> 2) * g.CS + 4 * q;
-      double acc[2][2][2][2];  // [row tile][colrow half][re/im][2 columns]
+      constexpr int NH = kCTF / 8;
+      double acc[2][NH][2][2];  // [row tile][colrow half][re/im][2 columns]
 #pragma unroll
       for (int t = 0; t < 2; ++t)
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < NH; ++h)
 #pragma unroll
           for (int pt = 0; pt < 2; ++pt) acc[t][h][pt][0] = acc[t][h][pt][1] = 0.0;
 #pragma unroll
@@ -181,7 +175,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
         const double2 a0 = *reinterpret_cast<const double2 *>(pa0 + kb);
         const double2 a1 = *reinterpret_cast<const double2 *>(pa1 + kb);
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
+        for (int h = 0; h < NH; ++h) {
           const double2 be = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb);      // latitude 8j + 2q
           const double2 bo = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb + 2);  // latitude 8j + 2q + 1
           mma884(acc[0][h][0], a0.x, be.x);
@@ -200,7 +194,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_fwd_pair(V2Args a)
         const int r = par + 2 * (16 * gi + 8 * t + (lane >> 2));
         if (r >= R) continue;
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
+        for (int h = 0; h < NH; ++h)
 #pragma unroll
           for (int e = 0; e < 2; ++e) {
             const int c = col0 + 8 * h + 2 * q + e;
@@ -352,7 +346,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
 size_t fwd_smem(int N, int J)
 {
   const Geo g = make_geo(N, J, true);
-  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * 2 * kCT * (size_t)g.CS);
+  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * kCTF * (size_t)g.CS);
 }
 size_t inv_smem(int N, int J)
 {
@@ -377,7 +371,8 @@ int launch_pair(const sht_plan *p, bool inverse, const double2 *in, int ncol, do
   int npairs = 0;
   int rc = get_pairs(p, &a.pairs, &npairs);
   if (rc) { set_error("legendre: pair table missing"); return rc; }
-  a.ntiles = (ncol + kCT - 1) / kCT;
+  const int ct = inverse ? kCT : kCTF;
+  a.ntiles = (ncol + ct - 1) / ct;
   a.nitems = npairs * a.ntiles;
   const size_t smem = inverse ? inv_smem(p->N, p->J) : fwd_smem(p->N, p->J);
   void (*kern)(V2Args) = nullptr;
