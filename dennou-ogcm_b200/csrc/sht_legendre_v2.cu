@@ -1,20 +1,23 @@
 // sht_legendre_v2.cu -- persistent FP64 Legendre contraction with paired bands.
 //
 // The triangular band of order m has N+2-m degrees.  Pairing m with N-m makes
-// every pair hold N+4 degrees.  A work item is (pair, 16 complex field-level
-// columns), so all items cost the same.  Each thread block is resident and
-// takes a contiguous slice of the pair-major item list.  So it reloads the
-// pair's Legendre rows (P) at most a few times, and the blocks finish
-// together.  The next item's data panel is fetched with cp.async while the
-// current one is contracted on the FP64 tensor path (mma.sync.m8n8k4.f64).
+// every pair hold N+4 degrees.  A work item is (pair, 8 (analysis) or 16
+// (synthesis) complex field-level columns), so all items cost the same.  Each
+// thread block is resident and takes a contiguous slice of the pair-major
+// item list.  So it reloads the pair's Legendre rows (P) at most a few times,
+// and the blocks finish together.  The products run on the FP64 tensor path
+// (mma.sync.m8n8k4.f64).  The analysis runs two blocks per SM, each with one
+// data panel, so one block's panel load overlaps the other's products; the
+// synthesis runs one block per SM and fetches the next item's panel with
+// cp.async while the current one is contracted.
 // Shared-memory row strides are chosen so that every 16-lane phase of a
 // fragment load touches 16 distinct double-word bank pairs:
 //   P rows (stride-2 rows of one parity):  PS = 2 (mod 8) doubles (synthesis,
 //     8-byte fragment loads), 4 (mod 8) (analysis, 16-byte fragment loads)
 //   data rows (columns of one panel):      CS = 8 (mod 16) doubles
 //   coefficient rows (stride-2 rows):      AS = 2 (mod 8) doubles
-// Used when a pair's P rows and two data panels fit in shared memory (T85 and
-// smaller); larger grids use the chunked kernels of sht_legendre.cu.
+// Used when a pair's P rows and the data panels fit in shared memory (T85 and
+// smaller); larger grids use the chunked kernels of sht_legendre_v3.cu.
 //
 // Analysis follows space_discretization.tex:197-200 and synthesis :212-216.
 // Symmetric and antisymmetric latitude halves use Pbar(-mu) = (-1)^{n-m} Pbar(mu);
