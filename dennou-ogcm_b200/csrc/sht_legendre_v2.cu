@@ -1,8 +1,8 @@
 // sht_legendre_v2.cu -- persistent FP64 Legendre contraction with paired bands.
 //
 // The triangular band of order m has N+2-m degrees.  Pairing m with N-m makes
-// every pair hold N+4 degrees.  A work item is (pair, 8 (analysis) or 16
-// (synthesis) complex field-level columns), so all items cost the same.  Each
+// every pair hold N+4 degrees.  A work item is (pair, 8 (analysis at JH = 64)
+// or 16 complex field-level columns), so all items cost the same.  Each
 // thread block is resident and takes a contiguous slice of the pair-major
 // item list.  So it reloads the pair's Legendre rows (P) at most a few times,
 // and the blocks finish together.  The products run on the FP64 tensor path
@@ -33,7 +33,9 @@ namespace {
 constexpr int kW = 8;            // warps per block
 constexpr int kT = kW * 32;      // threads per block
 constexpr int kCT = 16;          // complex columns per item (synthesis)
-constexpr int kCTF = 8;          // complex columns per item (analysis: one panel, two blocks per SM)
+// complex columns per analysis item: 8 at JH = 64 (one panel per block, two
+// blocks per SM), 16 below, where an item's contraction is short
+__host__ __device__ constexpr int ct_fwd(int JH) { return JH >= 64 ? 8 : 16; }
 
 struct Geo {
   int PS, CS, AS;      // strides (doubles)
@@ -100,11 +102,12 @@ template <int JH>
 __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
 {
   constexpr int J = 2 * JH, RSTEP = kT / J;  // column rows covered per pass
-  const int nrow = (mb >= 0) ? 2 * kCTF : kCTF;
+  constexpr int CT = ct_fwd(JH);
+  const int nrow = (mb >= 0) ? 2 * CT : CT;
   const int j = threadIdx.x % J;
 #pragma unroll 4
   for (int row = threadIdx.x / J; row < nrow; row += RSTEP) {
-    const int mi = row / kCTF, b = row % kCTF;
+    const int mi = row / CT, b = row % CT;
     const int m = mi ? mb : ma;
     const bool ok = col0 + b < a.ncol;
     const double2 *src = ok ? a.F + ((long long)m * a.ncol + col0 + b) * J + j : a.F;
@@ -128,7 +131,7 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
 
   int cur = -1;
   for (int it = it0; it < it1; ++it) {
-    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * kCTF;
+    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * ct_fwd(JH);
     const int2 pr = a.pairs[pidx];
     if (pidx != cur) {
       load_pair_P<JH>(a, g, Pbuf, pr.x, pr.y);
@@ -153,7 +156,7 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
       else { mi = 1; par = 1; gi = job - gEa - gOa - gEb; }
       const int m = mi ? pr.y : pr.x, R = mi ? Rb : Ra;
       const double *Pm = Pbuf + (mi ? Ra : 0) * g.PS;
-      const double *G = Gcur + mi * kCTF * g.CS + (par ? 2 * JH : 0);
+      const double *G = Gcur + mi * ct_fwd(JH) * g.CS + (par ? 2 * JH : 0);
       const int r0 = par + 2 * (16 * gi + (lane >> 2));
       const int r1 = r0 + 16;
       // K order within each pair of k-steps: lane q = lane & 3 takes latitude
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
       const double *pa0 = Pm + min(r0, R - 1) * g.PS + 2 * q;
       const double *pa1 = Pm + min(r1, R - 1) * g.PS + 2 * q;
       const double *gb = G + (lane >> 2) * g.CS + 4 * q;
-      constexpr int NH = kCTF / 8;
+      constexpr int NH = ct_fwd(JH) / 8;
       double acc[2][NH][2][2];  // [row tile][colrow half][re/im][2 columns]
 #pragma unroll
       for (int t = 0; t < 2; ++t)
@@ -349,7 +352,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
 size_t fwd_smem(int N, int J)
 {
   const Geo g = make_geo(N, J, true);
-  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * kCTF * (size_t)g.CS);
+  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * ct_fwd(J / 2) * (size_t)g.CS);
 }
 size_t inv_smem(int N, int J)
 {
@@ -374,7 +377,7 @@ int launch_pair(const sht_plan *p, bool inverse, const double2 *in, int ncol, do
   int npairs = 0;
   int rc = get_pairs(p, &a.pairs, &npairs);
   if (rc) { set_error("legendre: pair table missing"); return rc; }
-  const int ct = inverse ? kCT : kCTF;
+  const int ct = inverse ? kCT : ct_fwd(p->JH);
   a.ntiles = (ncol + ct - 1) / ct;
   a.nitems = npairs * a.ntiles;
   const size_t smem = inverse ? inv_smem(p->N, p->J) : fwd_smem(p->N, p->J);
