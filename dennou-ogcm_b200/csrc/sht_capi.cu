@@ -328,10 +328,12 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
     p->io_bytes = need;
   }
   double *d = static_cast<double *>(p->d_io);
-  double *di0 = d, *di1 = d + al(nin_each), *di2 = d + 2 * al(nin_each);
-  double *do0 = d + al(nin_each) * sh.nin, *do1 = do0 + al(nout_each);
+  // staging: the operator's inputs, then its outputs
   const double *hin[3] = {i0, i1, i2};
-  double *din[3] = {di0, di1, di2};
+  double *din[3] = {nullptr, nullptr, nullptr};
+  for (int k = 0; k < sh.nin; ++k) din[k] = d + k * al(nin_each);
+  double *const di0 = din[0];
+  double *do0 = d + al(nin_each) * sh.nin, *do1 = sh.nout == 2 ? do0 + al(nout_each) : nullptr;
   // device input k (or null past the operator's inputs), offset by `off` doubles
   auto dev_in = [&](int k, size_t off) -> const double * { return k < sh.nin ? din[k] + off : nullptr; };
   cudaStream_t s = p->stream;
