@@ -32,20 +32,9 @@ int cuda_fail(cudaError_t e, const char *what)
 }
 void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
-int device_error_status(sht_plan *p)
-{
-  int h = 0;
-  if (p->d_err) {
-    cudaError_t e = cudaMemcpy(&h, p->d_err, sizeof(int), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) return cuda_fail(e, "device error word");
-    if (h) {
-      cudaMemset(p->d_err, 0, sizeof(int));
-      set_error("a bounded device-side wait of the FP64 Legendre kernels timed out");
-      return h;
-    }
-  }
-  return split_error_status(p);
-}
+// The bounded device-side waits are those of the split-precision kernel; its
+// error word is read only once its tables exist.
+int device_error_status(sht_plan *p) { return split_error_status(p); }
 
 namespace {
 
@@ -306,6 +295,10 @@ int api_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, dou
   return rc;
 }
 
+// Calls whose host arrays total at most this many bytes and are pageable are
+// staged through page-locked host memory (per-level calls up to T341).
+constexpr size_t kPinnedStageMax = 8u << 20;
+
 int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
              const double *i2 = nullptr)
 {
@@ -350,15 +343,47 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
     for (auto &ev : p->chunk_ev)
       if ((e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming)) != cudaSuccess) return cuda_fail(e, "chunk events");
   }
+  // Small calls on pageable host arrays (one level at a time, as the
+  // reference's loops call) go through the plan's pinned staging buffer: a
+  // host memcpy plus an asynchronous copy costs less than the driver's
+  // pageable path.  Page-locked arrays are copied directly.
+  double *hs = nullptr;
   if (nchunk == 1) {
-    for (int k = 0; k < sh.nin; ++k)
-      if ((e = cudaMemcpyAsync(din[k], hin[k], sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    const size_t stage_bytes = sizeof(double) * (nin_each * sh.nin + nout_each * sh.nout);
+    bool pageable = false;
+    auto is_pageable = [](const void *ptr) {
+      cudaPointerAttributes at;
+      if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) { cudaGetLastError(); return true; }
+      return at.type == cudaMemoryTypeUnregistered;
+    };
+    for (int k = 0; k < sh.nin; ++k) pageable = pageable || is_pageable(hin[k]);
+    pageable = pageable || is_pageable(o0) || (sh.nout == 2 && is_pageable(o1));
+    if (pageable && stage_bytes <= kPinnedStageMax) {
+      if (stage_bytes > p->h_stage_bytes) {
+        if (p->h_stage) { cudaStreamSynchronize(s); cudaFreeHost(p->h_stage); p->h_stage = nullptr; p->h_stage_bytes = 0; }
+        if ((e = cudaMallocHost(&p->h_stage, stage_bytes)) != cudaSuccess) return cuda_fail(e, "cudaMallocHost(staging)");
+        p->h_stage_bytes = stage_bytes;
+      }
+      hs = static_cast<double *>(p->h_stage);
+    }
+  }
+  if (nchunk == 1) {
+    double *hso = hs ? hs + nin_each * sh.nin : nullptr;  // staged outputs
+    for (int k = 0; k < sh.nin; ++k) {
+      const double *src = hin[k];
+      if (hs) {
+        std::memcpy(hs + k * nin_each, hin[k], sizeof(double) * nin_each);
+        src = hs + k * nin_each;
+      }
+      if ((e = cudaMemcpyAsync(din[k], src, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
         return cuda_fail(e, "H2D");
+    }
     rc = run_dev(p, op, di0, dev_in(1, 0), nb, do0, sh.nout == 2 ? do1 : nullptr, dev_in(2, 0));
     if (rc) return rc;
-    if ((e = cudaMemcpyAsync(o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    if ((e = cudaMemcpyAsync(hs ? hso : o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return cuda_fail(e, "D2H");
-    if (sh.nout == 2 && (e = cudaMemcpyAsync(o1, do1, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    if (sh.nout == 2 && (e = cudaMemcpyAsync(hs ? hso + nout_each : o1, do1, sizeof(double) * nout_each,
+                                             cudaMemcpyDeviceToHost, s)) != cudaSuccess)
       return cuda_fail(e, "D2H");
   } else {
     const size_t pin = nin_each / nb, pout = nout_each / nb;  // doubles per field-level
@@ -388,6 +413,11 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
     if ((e = cudaStreamSynchronize(p->copy_out)) != cudaSuccess) return cuda_fail(e, "D2H");
   }
   if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
+  if (hs) {
+    const double *hso = hs + nin_each * sh.nin;
+    std::memcpy(o0, hso, sizeof(double) * nout_each);
+    if (sh.nout == 2) std::memcpy(o1, hso + nout_each, sizeof(double) * nout_each);
+  }
   if ((rc = device_error_status(p))) return rc;
   finish_timing(p, !sh.out_grid);
   return SHT_OK;
@@ -398,7 +428,8 @@ void free_plan(sht_plan *p)
   cudaFree(p->d_mu); cudaFree(p->d_wgt); cudaFree(p->d_rowscale); cudaFree(p->d_P);
   cudaFree(p->d_poff); cudaFree(p->d_rowoff); cudaFree(p->d_eps); cudaFree(p->d_tw);
   cudaFree(p->d_twI); cudaFree(p->d_rn); cudaFree(p->d_spec_tiles); cudaFree(p->d_pairs);
-  cudaFree(p->d_ws); cudaFree(p->d_io); cudaFree(p->d_err);
+  cudaFree(p->d_ws); cudaFree(p->d_io);
+  if (p->h_stage) cudaFreeHost(p->h_stage);
   free_split_tables(p);
   for (auto &ev : p->timing.ev)
     if (ev) cudaEventDestroy(ev);
@@ -516,8 +547,6 @@ int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
   cudaGetDevice(&p->device);
   int rc = SHT_OK;
   if ((e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking)) != cudaSuccess) rc = cuda_fail(e, "stream create");
-  if (!rc && ((e = cudaMalloc(&p->d_err, sizeof(int))) != cudaSuccess || (e = cudaMemset(p->d_err, 0, sizeof(int))) != cudaSuccess))
-    rc = cuda_fail(e, "error word");
   p->stream = p->own_stream;
   for (int k = 0; k < 8 && !rc; ++k)
     if ((e = cudaEventCreate(&p->timing.ev[k])) != cudaSuccess) rc = cuda_fail(e, "event create");

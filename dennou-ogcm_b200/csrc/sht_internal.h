@@ -105,11 +105,12 @@ struct sht_plan_s {
   // device staging for the host-pointer API, grown on demand
   void *d_io = nullptr;
   size_t io_bytes = 0;
+  // page-locked host staging for small host-pointer calls on pageable arrays
+  void *h_stage = nullptr;
+  size_t h_stage_bytes = 0;
 
   // split-precision tables (built lazily)
   void *tc_tables = nullptr;
-  // device error word of the bounded waits in the FP64 kernels (0 = none)
-  int *d_err = nullptr;
 
   std::mutex mtx;
   sht::Timing timing;
