@@ -177,6 +177,28 @@ def test_round_trip_property_large(grid, plans):
     assert relerr(gpu.wa_xya(gpu.xya_wa(w)), w) < TOL
 
 
+def test_largest_grid_properties():
+    """The largest longitude count a plan takes (im = 2048: the 1024-point
+    complex FFT) with 512 half-latitudes (beyond the paired and chunked
+    Legendre kernels, so the per-band ones run): a band-limited round trip is
+    the identity, and d/dlambda of a spectrum equals the synthesis of i m times
+    it.  The oracle is too slow at T682, so these are properties."""
+    N = 682
+    gpu = pkg().SpmlUtil(2048, 1024, 1, N)
+    try:
+        w = workloads().seeded_spectra(N, 2, 2.0, seed=5)
+        assert relerr(gpu.wa_xya(gpu.xya_wa(w)), w) < TOL
+        im_w = np.zeros_like(w)
+        for n in range(1, N + 1):
+            m = np.arange(1, n + 1)
+            c, s_ = n * (n + 1) + m, n * (n + 1) - m
+            im_w[:, c] = -m * w[:, s_]
+            im_w[:, s_] = m * w[:, c]
+        assert relerr(gpu.xya_GradLambda_wa(w), gpu.xya_wa(im_w)) < TOL
+    finally:
+        gpu.final()
+
+
 def test_device_pointer_path_matches_host(plans):
     import torch
     I, J, N = 256, 128, 85
