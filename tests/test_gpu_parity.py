@@ -249,6 +249,13 @@ def test_error_paths(plans):
     import ctypes
     buf = (ctypes.c_double * 8)()
     assert lib.sht_wa_xya(None, buf, 1, buf) == 3
+    # an empty batch is a no-op on a live plan, even with null arrays
+    assert lib.sht_wa_xya(gpu._h, None, 0, None) == 0
+    assert lib.sht_xya_wa_dev(gpu._h, None, 0, None) == 0
+    assert lib.sht_wa_alphaoptr_prod_xya(gpu._h, None, None, None, 0, None) == 0
+    # negative counts and null arrays with work to do are rejected
+    assert lib.sht_xya_wa(gpu._h, buf, -3, buf) == 1
+    assert lib.sht_xya_hgrad_wa(gpu._h, buf, 1, buf, None) == 1
 
 
 @pytest.mark.parametrize("grid", [(64, 32, 21), (128, 64, 42), (256, 128, 85), (256, 128, 84), (32, 32, 10),
