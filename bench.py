@@ -266,6 +266,55 @@ def bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world):
     return out
 
 
+def bench_operators(P, torch, dev, sht, args, flush, max_over_ranks, world):
+    """The SpmlUtil composites on the headline plan and batch, FP64, each as
+    one batched call, in transform-equivalents: the number of single-level
+    SPML transforms the reference spends per level (w_AlphaOptr_xy is
+    w_DivLambda_xy + w_DivMu_xy, two analyses; calc_UVCosLat2VorDiv two
+    AlphaOptr, four analyses; calc_VorDiv2UV four syntheses;
+    SpmlUtil_mod.f90:299-473).  CUDA events on the launching stream, L2
+    flushed between steps outside the events."""
+    nb = args.nb or 480
+    g = torch.Generator(device=dev).manual_seed(20261204)
+    shape = (nb, sht.jm, sht.im)
+    xa, xb = (torch.randn(shape, generator=g, dtype=torch.float64, device=dev) for _ in range(2))
+    wa = torch.randn((nb, sht.lm), generator=g, dtype=torch.float64, device=dev)
+    wb = torch.randn((nb, sht.lm), generator=g, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sht.set_precision(P.SHT_PREC_FP64)
+    ops = {  # name: (call, reference transforms per level)
+        "w_xy": (lambda: sht.w_xy(xa), 1),
+        "xy_w": (lambda: sht.xy_w(wa), 1),
+        "w_DivMu_xy": (lambda: sht.w_DivMu_xy(xa), 1),
+        "xy_GradLon_w": (lambda: sht.xy_GradLon_w(wa), 1),
+        "xy_GradLat_w": (lambda: sht.xy_GradLat_w(wa), 1),
+        "w_AlphaOptr_xy": (lambda: sht.w_AlphaOptr_xy(xa, xb), 2),
+        "xy_AlphaOptr_w": (lambda: sht.xy_AlphaOptr_w(wa, wb), 2),
+        "calc_UVCosLat2VorDiv": (lambda: sht.calc_UVCosLat2VorDiv(xa, xb), 4),
+        "calc_VorDiv2UV": (lambda: sht.calc_VorDiv2UV(wa, wb), 4),
+    }
+    out = {"workload": f"{nb} field-levels on the headline grid, fp64",
+           "unit": "transform-equivalents/s (reference single-level transforms per second)"}
+    for name, (fn, count) in ops.items():
+        for _ in range(max(args.warmup, 3)):
+            flush.zero_()
+            fn()
+        torch.cuda.synchronize()
+        tot = 0.0
+        for _ in range(args.steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            e1.synchronize()
+            tot += e0.elapsed_time(e1)
+        ms = max_over_ranks(tot) / args.steps
+        out[name] = {"ms": ms, "reference_transforms_per_level": count,
+                     "transform_equivalents_per_s": world * nb * count / (ms * 1e-3)}
+    return out
+
+
 def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
     """The fused clients against their unfused compositions on the headline
     plan and batch, FP64, CUDA events on the launching stream, L2 flushed
@@ -355,6 +404,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-multi", action="store_true", help="skip the C3 multi-instance measurement")
     ap.add_argument("--no-fused", action="store_true", help="skip the fused-client measurements")
+    ap.add_argument("--no-operators", action="store_true", help="skip the per-operator measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -525,6 +575,7 @@ def main():
 
     multi = None if args.no_multi else bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world)
     fused = None if args.no_fused else bench_fused(P, torch, dev, sht, args, flush, max_over_ranks)
+    operators = None if args.no_operators else bench_operators(P, torch, dev, sht, args, flush, max_over_ranks, world)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -552,6 +603,7 @@ def main():
             "gpu_launches": head["launches"],
             "multi_instance": multi,
             "fused_clients": fused,
+            "operators": operators,
         }
         print(json.dumps(rec))
     sht.final()
