@@ -295,6 +295,9 @@ int api_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, dou
   return rc;
 }
 
+int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
+              const double *i2);
+
 // Calls whose host arrays total at most this many bytes and are pageable are
 // staged through page-locked host memory (per-level calls up to T341).
 constexpr size_t kPinnedStageMax = 8u << 20;
@@ -307,6 +310,14 @@ int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, do
   std::lock_guard<std::mutex> lk(p->mtx);
   DeviceGuard g(p->device);
   if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
+  return host_call(p, op, i0, i1, nb, o0, o1, i2);
+}
+
+// the body of a host-pointer call (arguments checked, plan mutex held, device set)
+int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
+              const double *i2)
+{
+  int rc;
   const OpShape sh = shape_of(op);
   const size_t nin_each = sh.in_grid ? (size_t)nb * p->I * p->J : (size_t)nb * p->L;
   const size_t nout_each = out_count(p, op, nb);
@@ -461,6 +472,115 @@ int run_synthesis_cols(sht_plan *p, const double *const *wcol, int ncol, double 
   if ((rc = leg_inv(p, S, ncol, F, s))) return rc;
   return launch_fft_inv(p, F, ncol, 0, ncol, nullptr, nullptr, ncol, RS_INV_PLAIN, s, gcol);
 }
+
+namespace {
+
+int check_strided(const sht_plan *p, const void *g, int ldi, int ldj, int nb, const void *w, int ldw, int mode)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (nb < 0) { set_error("nb must be >= 0"); return SHT_ERR_INVALID_ARG; }
+  if (mode != -1 && mode != SHT_PREC_FP64 && mode != SHT_PREC_SPLIT) {
+    set_error("unknown precision mode");
+    return SHT_ERR_INVALID_ARG;
+  }
+  if (nb == 0) return SHT_OK;
+  if (!g || !w) { set_error("null array argument"); return SHT_ERR_INVALID_ARG; }
+  if (ldi < p->I || ldj < p->J || ldw < p->L) {
+    set_error("leading dimensions must be at least im, jm and lm");
+    return SHT_ERR_INVALID_ARG;
+  }
+  return SHT_OK;
+}
+
+// copies nb levels of an im x jm section (row pitch ldi, ldj rows per level)
+// to or from a contiguous im x jm x nb array
+cudaError_t copy_grid(const sht_plan *p, void *dst, int dst_ldi, int dst_ldj, const void *src, int src_ldi,
+                      int src_ldj, int nb, cudaMemcpyKind kind, cudaStream_t s)
+{
+  cudaMemcpy3DParms c = {};
+  c.srcPtr = make_cudaPitchedPtr(const_cast<void *>(src), sizeof(double) * src_ldi, sizeof(double) * p->I, src_ldj);
+  c.dstPtr = make_cudaPitchedPtr(dst, sizeof(double) * dst_ldi, sizeof(double) * p->I, dst_ldj);
+  c.extent = make_cudaExtent(sizeof(double) * p->I, p->J, nb);
+  c.kind = kind;
+  return cudaMemcpy3DAsync(&c, s);
+}
+
+// staging: grid (im jm nb) then spectra (lm nb), each on a 256-byte boundary
+int strided_staging(sht_plan *p, int nb, double **dg, double **dw)
+{
+  auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };
+  const size_t ng = (size_t)nb * p->I * p->J, nw = (size_t)nb * p->L;
+  const size_t need = sizeof(double) * (al(ng) + al(nw)) + 1024;
+  if (need > p->io_bytes) {
+    cudaError_t e;
+    if (p->d_io) { cudaStreamSynchronize(p->stream); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
+    if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
+    p->io_bytes = need;
+  }
+  *dg = static_cast<double *>(p->d_io);
+  *dw = *dg + al(ng);
+  return SHT_OK;
+}
+
+// The plan's precision for one call (mode -1 keeps it), restored on scope exit.
+struct PrecisionScope {
+  sht_plan *p;
+  int saved;
+  PrecisionScope(sht_plan *plan, int mode) : p(plan), saved(plan->precision)
+  {
+    if (mode >= 0) p->precision = mode;
+  }
+  ~PrecisionScope() { p->precision = saved; }
+};
+
+int strided_call(sht_plan *p, bool analysis, const double *g_in, double *g_out, int ldi, int ldj, int nb,
+                 const double *w_in, double *w_out, int ldw, int mode, bool host)
+{
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard guard(p->device);
+  if (!guard.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
+  PrecisionScope ps(p, mode);
+  int rc;
+  if (ldi == p->I && ldj == p->J && ldw == p->L) {  // contiguous: the ordinary call
+    const int op = analysis ? OP_W_XY : OP_XY_W;
+    const double *in = analysis ? g_in : w_in;
+    double *out = analysis ? w_out : g_out;
+    if (host) return host_call(p, op, in, nullptr, nb, out, nullptr, nullptr);
+    if ((rc = check_dev_alignment(op, in, nullptr, out, nullptr))) return rc;
+    if ((rc = run_dev(p, op, in, nullptr, nb, out, nullptr))) return rc;
+    finish_timing(p, analysis);
+    return SHT_OK;
+  }
+  cudaStream_t s = p->stream;
+  const cudaMemcpyKind to_dev = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind from_dev = host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  double *dg = nullptr, *dw = nullptr;
+  rc = strided_staging(p, nb, &dg, &dw);
+  if (rc) return rc;
+  cudaError_t e;
+  if (analysis) {
+    if ((e = copy_grid(p, dg, p->I, p->J, g_in, ldi, ldj, nb, to_dev, s)) != cudaSuccess) return cuda_fail(e, "grid copy in");
+    if ((rc = run_dev(p, OP_W_XY, dg, nullptr, nb, dw, nullptr))) return rc;
+    if ((e = cudaMemcpy2DAsync(w_out, sizeof(double) * ldw, dw, sizeof(double) * p->L, sizeof(double) * p->L, nb,
+                               from_dev, s)) != cudaSuccess)
+      return cuda_fail(e, "spectral copy out");
+  } else {
+    if ((e = cudaMemcpy2DAsync(dw, sizeof(double) * p->L, w_in, sizeof(double) * ldw, sizeof(double) * p->L, nb,
+                               to_dev, s)) != cudaSuccess)
+      return cuda_fail(e, "spectral copy in");
+    if ((rc = run_dev(p, OP_XY_W, dw, nullptr, nb, dg, nullptr))) return rc;
+    if ((e = copy_grid(p, g_out, ldi, ldj, dg, p->I, p->J, nb, from_dev, s)) != cudaSuccess) return cuda_fail(e, "grid copy out");
+  }
+  if (host) {
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
+    if ((rc = device_error_status(p))) return rc;
+  }
+  finish_timing(p, analysis);
+  return SHT_OK;
+}
+
+}  // namespace
 
 }  // namespace sht
 
@@ -752,6 +872,42 @@ int sht_vordiv2uv(sht_plan *p, const double *vor, const double *div, int nb, dou
 { return api_host(p, OP_VORDIV2UV, vor, div, nb, u, v); }
 int sht_vordiv2uv_dev(sht_plan *p, const double *vor, const double *div, int nb, double *u, double *v)
 { return api_dev(p, OP_VORDIV2UV, vor, div, nb, u, v); }
+
+// ---------------------------------------------------------------- strided
+// Analysis and synthesis of arrays with leading dimensions: the model keeps
+// its fields with halos, xyz(IA, JA, KA) with the transform's points at
+// (IS:IE, JS:JE) of every level, and copies each section in and out around
+// every SpmlUtil call (explicit-shape dummies).  These entry points take the
+// whole array instead: grid point (i, j) of level k at
+// xya[i + ldi (j + ldj k)], spectral entry l of level k at wa[l + ldw k].
+// The section moves between the caller's array and the contiguous staging by
+// pitched copies (cudaMemcpy3DAsync / cudaMemcpy2DAsync, one per array);
+// the transform itself is the ordinary batched one.
+
+int sht_analysis(sht_plan *p, const double *xya, int ldi, int ldj, int nb, double *wa, int ldw, int mode)
+{
+  int rc = check_strided(p, xya, ldi, ldj, nb, wa, ldw, mode);
+  if (rc || nb == 0) return rc;
+  return strided_call(p, true, xya, nullptr, ldi, ldj, nb, nullptr, wa, ldw, mode, true);
+}
+int sht_analysis_dev(sht_plan *p, const double *xya, int ldi, int ldj, int nb, double *wa, int ldw, int mode)
+{
+  int rc = check_strided(p, xya, ldi, ldj, nb, wa, ldw, mode);
+  if (rc || nb == 0) return rc;
+  return strided_call(p, true, xya, nullptr, ldi, ldj, nb, nullptr, wa, ldw, mode, false);
+}
+int sht_synthesis(sht_plan *p, const double *wa, int ldw, int nb, double *xya, int ldi, int ldj, int mode)
+{
+  int rc = check_strided(p, xya, ldi, ldj, nb, wa, ldw, mode);
+  if (rc || nb == 0) return rc;
+  return strided_call(p, false, nullptr, xya, ldi, ldj, nb, wa, nullptr, ldw, mode, true);
+}
+int sht_synthesis_dev(sht_plan *p, const double *wa, int ldw, int nb, double *xya, int ldi, int ldj, int mode)
+{
+  int rc = check_strided(p, xya, ldi, ldj, nb, wa, ldw, mode);
+  if (rc || nb == 0) return rc;
+  return strided_call(p, false, nullptr, xya, ldi, ldj, nb, wa, nullptr, ldw, mode, false);
+}
 
 static int diffuse_impl(sht_plan *p, double *w, int nb, const double *coef, double dt, const double *filter, bool host)
 {

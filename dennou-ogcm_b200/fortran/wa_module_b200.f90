@@ -32,6 +32,7 @@ module wa_module_b200
   public :: b200_calc_UVCosLat2VorDiv, b200_calc_VorDiv2UV
   public :: b200_wa_Diffuse
   public :: b200_wa_AlphaOptrProd_xya, b200_xya_HGrad_wa, b200_xya_HGrad_xya, b200_xya_FluxDiv_xya
+  public :: b200_wa_xyz_section, b200_xyz_wa_section
 
   integer, parameter :: SHT_OK = 0
   character(*), parameter :: module_name = 'wa_module_b200'
@@ -186,6 +187,21 @@ module wa_module_b200
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: plan; real(c_double), intent(in) :: a(*), b(*)
       integer(c_int), value :: nb; real(c_double), intent(out) :: x(*)
+    end function
+    integer(c_int) function sht_analysis(plan, x, ldi, ldj, nb, w, ldw, mode) bind(C, name='sht_analysis')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan, x
+      integer(c_int), value :: ldi, ldj, nb
+      real(c_double), intent(out) :: w(*)
+      integer(c_int), value :: ldw, mode
+    end function
+    integer(c_int) function sht_synthesis(plan, w, ldw, nb, x, ldi, ldj, mode) bind(C, name='sht_synthesis')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan
+      real(c_double), intent(in) :: w(*)
+      integer(c_int), value :: ldw, nb
+      type(c_ptr), value :: x
+      integer(c_int), value :: ldi, ldj, mode
     end function
     integer(c_int) function sht_wa_diffuse(plan, w, nb, coef, dt, filt) bind(C, name='sht_wa_diffuse')
       import :: c_int, c_double, c_ptr
@@ -457,5 +473,41 @@ contains
     call check(sht_xya_fluxdiv_xya(plan, xya_A, xya_B, int(size(xya_A, 3), c_int), b200_xya_FluxDiv_xya), &
          'xya_FluxDiv_xya')
   end function b200_xya_FluxDiv_xya
+
+  !> wa_xya of the section xyz(is:is+im-1, js:js+jm-1, :) of a haloed array
+  !> xyz(IA, JA, KA) (util/grid/DOGCM_GaussSpmVFvmGrid_mod.f90:158-183; with
+  !> the model's one-point halos is = js = 2), read in place through the
+  !> array's leading dimensions instead of an explicit-shape section copy.
+  !> mode: SHT_PREC_FP64 / SHT_PREC_SPLIT for this call (default: the plan's).
+  function b200_wa_xyz_section(xyz, is, js, mode)
+    real(DP), intent(in), contiguous, target :: xyz(:,:,:)
+    integer, intent(in) :: is, js
+    integer, intent(in), optional :: mode
+    real(DP) :: b200_wa_xyz_section(lm, size(xyz, 3))
+    integer(c_int) :: md
+    md = -1
+    if (present(mode)) md = int(mode, c_int)
+    if (is < 1 .or. js < 1 .or. is + im - 1 > size(xyz, 1) .or. js + jm - 1 > size(xyz, 2)) &
+         call MessageNotify('E', module_name, 'wa_xyz_section: section outside the array')
+    call check(sht_analysis(plan, c_loc(xyz(is, js, 1)), int(size(xyz, 1), c_int), int(size(xyz, 2), c_int), &
+         int(size(xyz, 3), c_int), b200_wa_xyz_section, int(lm, c_int), md), 'wa_xyz_section')
+  end function b200_wa_xyz_section
+
+  !> xya_wa into the section xyz(is:is+im-1, js:js+jm-1, :) of a haloed array;
+  !> the halo points keep their values.  wa(LW, KA) with LW >= lm.
+  subroutine b200_xyz_wa_section(wa, xyz, is, js, mode)
+    real(DP), intent(in) :: wa(:,:)
+    real(DP), intent(inout), contiguous, target :: xyz(:,:,:)
+    integer, intent(in) :: is, js
+    integer, intent(in), optional :: mode
+    integer(c_int) :: md
+    md = -1
+    if (present(mode)) md = int(mode, c_int)
+    if (is < 1 .or. js < 1 .or. is + im - 1 > size(xyz, 1) .or. js + jm - 1 > size(xyz, 2) .or. &
+         size(wa, 2) /= size(xyz, 3)) &
+         call MessageNotify('E', module_name, 'xyz_wa_section: section outside the array')
+    call check(sht_synthesis(plan, wa, int(size(wa, 1), c_int), int(size(wa, 2), c_int), c_loc(xyz(is, js, 1)), &
+         int(size(xyz, 1), c_int), int(size(xyz, 2), c_int), md), 'xyz_wa_section')
+  end subroutine b200_xyz_wa_section
 
 end module wa_module_b200

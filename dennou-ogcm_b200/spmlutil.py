@@ -101,6 +101,11 @@ def load_library(path: str | None = None):
         getattr(lib, "sht_wa_alphaoptr_prod_xya" + suf).argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int, _VP]
     for suf in ("", "_dev"):
         getattr(lib, "sht_wa_diffuse" + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
+    for suf in ("", "_dev"):
+        getattr(lib, "sht_analysis" + suf).argtypes = [_VP, _VP, ctypes.c_int, ctypes.c_int, ctypes.c_int, _VP,
+                                                       ctypes.c_int, ctypes.c_int]
+        getattr(lib, "sht_synthesis" + suf).argtypes = [_VP, _VP, ctypes.c_int, ctypes.c_int, _VP, ctypes.c_int,
+                                                        ctypes.c_int, ctypes.c_int]
     lib.sht_roundtrip_diffuse_dev.argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
     lib.sht_plan_l_nm.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
     lib.sht_plan_nm_l.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]
@@ -419,6 +424,78 @@ class SpmlUtil:
             st = lib.sht_wa_diffuse(self._h, _VP(out.ctypes.data), nb, _VP(c.ctypes.data), float(dt),
                                     _VP(f.ctypes.data) if f is not None else None)
         _check(st, "diffuse")
+        return out
+
+    # ------------------------------------ haloed arrays (leading dimensions)
+    def _section(self, x, i0, j0, name):
+        """(pointer to point (i0, j0) of level 0, ldi, ldj, nb, device?) of a
+        C-contiguous (nb, JA, IA) or (JA, IA) array holding an im x jm section."""
+        if x.ndim not in (2, 3):
+            raise SpmlError(1, name, "grid array must be (JA, IA) or (nb, JA, IA)")
+        ja, ia = int(x.shape[-2]), int(x.shape[-1])
+        nb = int(x.shape[0]) if x.ndim == 3 else 1
+        if i0 < 0 or j0 < 0 or i0 + self.im > ia or j0 + self.jm > ja:
+            raise SpmlError(1, name, f"section ({i0}, {j0}) + ({self.im}, {self.jm}) exceeds ({ia}, {ja})")
+        off = 8 * (j0 * ia + i0)
+        if _is_torch_cuda(x):
+            import torch
+            if x.dtype != torch.float64 or not x.is_contiguous():
+                raise SpmlError(1, name, "device grid array must be a contiguous float64 tensor")
+            return x.data_ptr() + off, ia, ja, nb, True
+        if x.dtype != np.float64 or not x.flags.c_contiguous:
+            raise SpmlError(1, name, "grid array must be a C-contiguous float64 array")
+        return x.ctypes.data + off, ia, ja, nb, False
+
+    def _spec_rows(self, w, nb, dev, name):
+        """(pointer, ldw) of a C-contiguous (nb, LW) spectral array, LW >= lm."""
+        if w.ndim != 2 or int(w.shape[0]) != nb or int(w.shape[1]) < self.lm:
+            raise SpmlError(1, name, f"spectral array must be ({nb}, >= {self.lm}), got {tuple(w.shape)}")
+        if dev != _is_torch_cuda(w):
+            raise SpmlError(1, name, "grid and spectral arrays must both be host or both be device arrays")
+        if dev:
+            import torch
+            if w.dtype != torch.float64 or not w.is_contiguous():
+                raise SpmlError(1, name, "device spectral array must be a contiguous float64 tensor")
+            return w.data_ptr(), int(w.shape[1])
+        if w.dtype != np.float64 or not w.flags.c_contiguous:
+            raise SpmlError(1, name, "spectral array must be a C-contiguous float64 array")
+        return w.ctypes.data, int(w.shape[1])
+
+    def analysis(self, xya, i0: int = 0, j0: int = 0, out=None, mode: int = -1):
+        """w_xy of the im x jm section at (i0, j0) of each level of a haloed
+        array (nb, JA, IA), e.g. i0 = j0 = 1 for the model's one-point halos;
+        out: (nb, LW >= lm) array for the spectra (allocated if None); mode:
+        precision for this call (-1: the plan's)."""
+        lib = load_library()
+        ptr, ldi, ldj, nb, dev = self._section(xya, i0, j0, "analysis")
+        if out is None:
+            if dev:
+                import torch
+                out = torch.empty((nb, self.lm), dtype=torch.float64, device=xya.device)
+            else:
+                out = np.empty((nb, self.lm))
+        wp, ldw = self._spec_rows(out, nb, dev, "analysis")
+        if dev:
+            self._set_torch_stream(xya)
+            st = lib.sht_analysis_dev(self._h, _VP(ptr), ldi, ldj, nb, _VP(wp), ldw, mode)
+        else:
+            st = lib.sht_analysis(self._h, _VP(ptr), ldi, ldj, nb, _VP(wp), ldw, mode)
+        _check(st, "analysis")
+        return out
+
+    def synthesis(self, wa, out, i0: int = 0, j0: int = 0, mode: int = -1):
+        """xy_w into the im x jm section at (i0, j0) of each level of the haloed
+        array out (nb, JA, IA); its other points are left as they are.  wa:
+        (nb, LW >= lm)."""
+        lib = load_library()
+        ptr, ldi, ldj, nb, dev = self._section(out, i0, j0, "synthesis")
+        wp, ldw = self._spec_rows(wa, nb, dev, "synthesis")
+        if dev:
+            self._set_torch_stream(out)
+            st = lib.sht_synthesis_dev(self._h, _VP(wp), ldw, nb, _VP(ptr), ldi, ldj, mode)
+        else:
+            st = lib.sht_synthesis(self._h, _VP(wp), ldw, nb, _VP(ptr), ldi, ldj, mode)
+        _check(st, "synthesis")
         return out
 
     def roundtrip_diffuse_(self, xya, coef=None, dt: float = 0.0, filt=None):

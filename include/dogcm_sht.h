@@ -264,6 +264,33 @@ SHT_API int sht_ya_intlon_xya_dev(sht_plan *plan, const double *xya, int nb, dou
 SHT_API int sht_roundtrip_diffuse_dev(sht_plan *plan, double *xya, int nb, const double *coef,
                               double dt, const double *filter);
 
+/* ------------------------------------------------- arrays with leading dimensions */
+
+/* Analysis (w_xy) and synthesis (xy_w) of haloed or padded arrays, with the
+ * precision chosen per call.  The model keeps its fields as xyz(IA, JA, KA)
+ * with halos (IHALO = JHALO = 1, util/grid/DOGCM_GaussSpmVFvmGrid_mod.f90:
+ * 158-183) and its loops copy the (IS:IE, JS:JE) section in and out of every
+ * SpmlUtil call through explicit-shape dummies (SpmlUtil_mod.f90:110, with
+ * the per-level loops of HBEBaroc_hspm_vfvm_mod.f90:160-172).  Here the
+ * caller passes the section's first point and the array's leading
+ * dimensions instead: grid point (i, j) of level k at
+ * xya[i + ldi*(j + ldj*k)] (0 <= i < im, 0 <= j < jm, ldi >= im, ldj >= jm),
+ * spectral entry l of level k at wa[l + ldw*k] (ldw >= lm).  Points outside
+ * the section (halos, padding) are neither read nor written.  mode is
+ * SHT_PREC_FP64 or SHT_PREC_SPLIT for this call only, or -1 for the plan's
+ * precision.  With ldi = im, ldj = jm, ldw = lm these are sht_wa_xya /
+ * sht_xya_wa (and their _dev forms); otherwise the sections move by pitched
+ * copies to and from the plan's staging.  The _dev forms take device
+ * pointers and run on the plan's stream without a final synchronisation. */
+SHT_API int sht_analysis(sht_plan *plan, const double *xya, int ldi, int ldj, int nb,
+                         double *wa, int ldw, int mode);
+SHT_API int sht_synthesis(sht_plan *plan, const double *wa, int ldw, int nb,
+                          double *xya, int ldi, int ldj, int mode);
+SHT_API int sht_analysis_dev(sht_plan *plan, const double *xya, int ldi, int ldj, int nb,
+                             double *wa, int ldw, int mode);
+SHT_API int sht_synthesis_dev(sht_plan *plan, const double *wa, int ldw, int nb,
+                              double *xya, int ldi, int ldj, int mode);
+
 /* ------------------------------------------------- analysis without allocation */
 
 /* No counterpart in the reference: this entry point exists for callers that

@@ -30,6 +30,23 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_fortran_shim_binds_declared_symbols():
+    """Every bind(C) interface of the Fortran front end names a declared entry
+    point, with as many arguments as the C declaration (no Fortran compiler
+    here, so this is the shim's link check)."""
+    shim = open(os.path.join(ROOT, "dennou-ogcm_b200", "fortran", "wa_module_b200.f90")).read()
+    binds = re.findall(r"function\s+(\w+)\s*\(([^)]*)\)\s*bind\(C,\s*name='(\w+)'\)", shim)
+    assert len(binds) >= 30
+    hdr = open(HEADER).read()
+    syms = set(declared_symbols())
+    for fname, args, cname in binds:
+        assert fname == cname and cname in syms, cname
+        decl = re.search(r"^SHT_API [^;]*?\b" + cname + r"\s*\(([^)]*)\)", hdr, flags=re.M).group(1)
+        n_c = 0 if decl.strip() in ("", "void") else decl.count(",") + 1
+        n_f = 0 if not args.strip() else args.count(",") + 1
+        assert n_c == n_f, (cname, n_c, n_f)
+
+
 def test_index_maps_and_status_text():
     p = pkg()
     assert p.l_nm(0, 0) == 1
@@ -71,6 +88,18 @@ def test_fused_clients_check_arguments_on_the_host():
     assert lib.sht_xya_hgrad_wa(None, buf, 1, buf, buf) == 3
     assert lib.sht_xya_hgrad_xya_dev(None, buf, 1, buf, buf) == 3
     assert lib.sht_xya_fluxdiv_xya(None, buf, buf, 1, buf) == 3
+
+
+def test_strided_calls_check_arguments_on_the_host():
+    """The leading-dimension entry points reject a null plan (whatever the
+    other arguments) before any device work."""
+    lib = pkg().load_library()
+    buf = (ctypes.c_double * 8)()
+    ptr = ctypes.cast(buf, ctypes.c_void_p)
+    assert lib.sht_analysis(None, ptr, 66, 34, 1, ptr, 500, -1) == 3
+    assert lib.sht_analysis_dev(None, ptr, 66, 34, 1, ptr, 500, 1) == 3
+    assert lib.sht_synthesis(None, ptr, 500, 1, ptr, 66, 34, 0) == 3
+    assert lib.sht_synthesis_dev(None, ptr, 500, 0, ptr, 66, 34, -1) == 3
 
 
 def test_init_without_device_reports_no_device(cuda_available):
