@@ -30,7 +30,50 @@ int cuda_fail(cudaError_t e, const char *what)
   if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return SHT_ERR_NO_DEVICE;
   return SHT_ERR_CUDA;
 }
-void count_launch(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+// this thread's launches, for the kernel count of a graph it captures
+static thread_local long long t_launches = 0;
+
+void count_launch(int n)
+{
+  g_launches.fetch_add(n, std::memory_order_relaxed);
+  t_launches += n;
+}
+
+cudaError_t kernel_setup(const void *kern, size_t smem, int threads, int *per_sm)
+{
+  struct Opt { int dev; const void *k; size_t max_smem; };
+  struct Occ { int dev; const void *k; size_t smem; int threads, blocks; };
+  static std::mutex mu;
+  static std::vector<Opt> opts;
+  static std::vector<Occ> occs;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (smem > 48 * 1024) {
+    Opt *o = nullptr;
+    for (Opt &c : opts)
+      if (c.dev == dev && c.k == kern) o = &c;
+    if (!o || o->max_smem < smem) {
+      // raised under the lock, so a concurrent smaller request cannot lower it
+      if ((e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
+        return e;
+      if (o) o->max_smem = smem;
+      else opts.push_back({dev, kern, smem});
+    }
+  }
+  if (!per_sm) return cudaSuccess;
+  for (const Occ &c : occs)
+    if (c.dev == dev && c.k == kern && c.smem == smem && c.threads == threads) {
+      *per_sm = c.blocks;
+      return cudaSuccess;
+    }
+  int blocks = 0;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, kern, threads, smem)) != cudaSuccess) return e;
+  occs.push_back({dev, kern, smem, threads, blocks});
+  *per_sm = blocks;
+  return cudaSuccess;
+}
 
 // The bounded device-side waits are those of the split-precision kernel; its
 // error word is read only once its tables exist.
@@ -85,6 +128,7 @@ int ensure_ws(sht_plan *p, int ncol, int nb_temp, Workspace *ws)
       p->d_ws = nullptr;
       p->ws_bytes = 0;
     }
+    ++p->buf_gen;
     cudaError_t e = cudaMalloc(&p->d_ws, need);
     if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(workspace)");
     p->ws_bytes = need;
@@ -301,6 +345,93 @@ int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, d
 // Calls whose host arrays total at most this many bytes and are pageable are
 // staged through page-locked host memory (per-level calls up to T341).
 constexpr size_t kPinnedStageMax = 8u << 20;
+constexpr size_t kMaxHostGraphs = 32;
+
+// Runs the device half of a staged host call (enqueue) as a CUDA graph.  The
+// first call of an (operator, size, precision, kernel choice) runs directly
+// and allocates whatever the operator needs; the second is captured on the
+// plan's capture stream and instantiated; later ones replay it, one graph
+// launch instead of two copies and three to six kernel launches.  Graphs
+// made before a plan buffer was reallocated are dropped.  A capture that the
+// runtime refuses leaves that key on the direct path.
+template <typename Enqueue>
+int host_graph_call(sht_plan *p, int op, int nb, Enqueue &&enqueue)
+{
+  cudaStream_t s = p->stream;
+  auto &gs = p->graphs;
+  for (size_t i = 0; i < gs.size();) {
+    if (gs[i].gen != p->buf_gen) {
+      if (gs[i].exec) cudaGraphExecDestroy(gs[i].exec);
+      gs.erase(gs.begin() + (long)i);
+    } else {
+      ++i;
+    }
+  }
+  HostGraph *g = nullptr;
+  for (HostGraph &c : gs)
+    if (c.op == op && c.nb == nb && c.precision == p->precision && c.leg_kernel == p->leg_kernel) g = &c;
+  cudaError_t e;
+  if (g && g->exec) {
+    if ((e = cudaGraphLaunch(g->exec, s)) != cudaSuccess) return cuda_fail(e, "graph launch");
+    count_launch(g->launches);
+    return SHT_OK;
+  }
+  if (!g || g->failed) {
+    if (!g) {
+      if (gs.size() >= kMaxHostGraphs) {
+        if (gs.front().exec) cudaGraphExecDestroy(gs.front().exec);
+        gs.erase(gs.begin());
+      }
+      HostGraph n;
+      n.op = op; n.nb = nb; n.precision = p->precision; n.leg_kernel = p->leg_kernel; n.gen = p->buf_gen;
+      gs.push_back(n);
+    }
+    return enqueue(s);
+  }
+  if (!p->cap_stream && cudaStreamCreateWithFlags(&p->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+    cudaGetLastError();
+    p->cap_stream = nullptr;
+    g->failed = true;
+    return enqueue(s);
+  }
+  const unsigned long long gen0 = p->buf_gen;
+  const long long n0 = t_launches;
+  if ((e = cudaStreamBeginCapture(p->cap_stream, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) {
+    cudaGetLastError();
+    g->failed = true;
+    return enqueue(s);
+  }
+  p->stream = p->cap_stream;
+  int rc = enqueue(p->cap_stream);
+  p->stream = s;
+  cudaGraph_t graph = nullptr;
+  e = cudaStreamEndCapture(p->cap_stream, &graph);
+  const int captured = (int)(t_launches - n0);  // recorded into the graph, not run
+  g_launches.fetch_sub(captured, std::memory_order_relaxed);
+  t_launches = n0;
+  cudaGraphExec_t exec = nullptr;
+  if (rc == SHT_OK && e == cudaSuccess && graph && p->buf_gen == gen0) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  // g may have moved if the list changed; find the entry again
+  g = nullptr;
+  for (HostGraph &c : gs)
+    if (c.op == op && c.nb == nb && c.precision == p->precision && c.leg_kernel == p->leg_kernel) g = &c;
+  if (rc != SHT_OK || e != cudaSuccess || !exec) {
+    cudaGetLastError();
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g) g->failed = true;
+    return enqueue(s);  // nothing captured has run
+  }
+  if (!g) {
+    cudaGraphExecDestroy(exec);
+    return enqueue(s);
+  }
+  g->exec = exec;
+  g->launches = captured;
+  if ((e = cudaGraphLaunch(exec, s)) != cudaSuccess) return cuda_fail(e, "graph launch");
+  count_launch(g->launches);
+  return SHT_OK;
+}
 
 int api_host(sht_plan *p, int op, const double *i0, const double *i1, int nb, double *o0, double *o1,
              const double *i2 = nullptr)
@@ -327,6 +458,7 @@ int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, d
   const size_t need = sizeof(double) * (al(nin_each) * sh.nin + al(nout_each) * sh.nout) + 1024;
   cudaError_t e;
   if (need > p->io_bytes) {
+    ++p->buf_gen;
     if (p->d_io) { cudaStreamSynchronize(p->stream); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
     if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
     p->io_bytes = need;
@@ -371,6 +503,7 @@ int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, d
     pageable = pageable || is_pageable(o0) || (sh.nout == 2 && is_pageable(o1));
     if (pageable && stage_bytes <= kPinnedStageMax) {
       if (stage_bytes > p->h_stage_bytes) {
+        ++p->buf_gen;
         if (p->h_stage) { cudaStreamSynchronize(s); cudaFreeHost(p->h_stage); p->h_stage = nullptr; p->h_stage_bytes = 0; }
         if ((e = cudaMallocHost(&p->h_stage, stage_bytes)) != cudaSuccess) return cuda_fail(e, "cudaMallocHost(staging)");
         p->h_stage_bytes = stage_bytes;
@@ -380,22 +513,27 @@ int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, d
   }
   if (nchunk == 1) {
     double *hso = hs ? hs + nin_each * sh.nin : nullptr;  // staged outputs
-    for (int k = 0; k < sh.nin; ++k) {
-      const double *src = hin[k];
-      if (hs) {
-        std::memcpy(hs + k * nin_each, hin[k], sizeof(double) * nin_each);
-        src = hs + k * nin_each;
-      }
-      if ((e = cudaMemcpyAsync(din[k], src, sizeof(double) * nin_each, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-        return cuda_fail(e, "H2D");
-    }
-    rc = run_dev(p, op, di0, dev_in(1, 0), nb, do0, sh.nout == 2 ? do1 : nullptr, dev_in(2, 0));
+    if (hs)
+      for (int k = 0; k < sh.nin; ++k) std::memcpy(hs + k * nin_each, hin[k], sizeof(double) * nin_each);
+    // the device half of the call on stream q (the plan's stream during it)
+    auto enqueue = [&](cudaStream_t q) -> int {
+      cudaError_t ee;
+      for (int k = 0; k < sh.nin; ++k)
+        if ((ee = cudaMemcpyAsync(din[k], hs ? hs + k * nin_each : hin[k], sizeof(double) * nin_each,
+                                  cudaMemcpyHostToDevice, q)) != cudaSuccess)
+          return cuda_fail(ee, "H2D");
+      int r = run_dev(p, op, di0, dev_in(1, 0), nb, do0, sh.nout == 2 ? do1 : nullptr, dev_in(2, 0));
+      if (r) return r;
+      if ((ee = cudaMemcpyAsync(hs ? hso : o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, q)) != cudaSuccess)
+        return cuda_fail(ee, "D2H");
+      if (sh.nout == 2 && (ee = cudaMemcpyAsync(hs ? hso + nout_each : o1, do1, sizeof(double) * nout_each,
+                                                cudaMemcpyDeviceToHost, q)) != cudaSuccess)
+        return cuda_fail(ee, "D2H");
+      return SHT_OK;
+    };
+    // staged calls name only plan buffers, so they can replay as graphs
+    rc = (hs && p->host_graphs && !p->timing.on) ? host_graph_call(p, op, nb, enqueue) : enqueue(s);
     if (rc) return rc;
-    if ((e = cudaMemcpyAsync(hs ? hso : o0, do0, sizeof(double) * nout_each, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-      return cuda_fail(e, "D2H");
-    if (sh.nout == 2 && (e = cudaMemcpyAsync(hs ? hso + nout_each : o1, do1, sizeof(double) * nout_each,
-                                             cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-      return cuda_fail(e, "D2H");
   } else {
     const size_t pin = nin_each / nb, pout = nout_each / nb;  // doubles per field-level
     // the plan stream and the copy streams start after any earlier work on the plan stream
@@ -442,6 +580,10 @@ void free_plan(sht_plan *p)
   cudaFree(p->d_ws); cudaFree(p->d_io);
   if (p->h_stage) cudaFreeHost(p->h_stage);
   free_split_tables(p);
+  for (auto &g : p->graphs)
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+  p->graphs.clear();
+  if (p->cap_stream) cudaStreamDestroy(p->cap_stream);
   for (auto &ev : p->timing.ev)
     if (ev) cudaEventDestroy(ev);
   if (p->own_stream) cudaStreamDestroy(p->own_stream);
@@ -514,6 +656,7 @@ int strided_staging(sht_plan *p, int nb, double **dg, double **dw)
   const size_t need = sizeof(double) * (al(ng) + al(nw)) + 1024;
   if (need > p->io_bytes) {
     cudaError_t e;
+    ++p->buf_gen;
     if (p->d_io) { cudaStreamSynchronize(p->stream); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
     if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
     p->io_bytes = need;
@@ -767,6 +910,10 @@ int sht_set_option(sht_plan *p, int option, int value)
     if (value < 0 || value > 3) { set_error("legendre kernel option must be 0, 1, 2 or 3"); return SHT_ERR_INVALID_ARG; }
     p->leg_kernel = value;
     return SHT_OK;
+  case SHT_OPT_HOST_GRAPHS:
+    if (value != 0 && value != 1) { set_error("host graphs option must be 0 or 1"); return SHT_ERR_INVALID_ARG; }
+    p->host_graphs = value == 1;
+    return SHT_OK;
   default: set_error("unknown option"); return SHT_ERR_INVALID_ARG;
   }
 }
@@ -778,6 +925,14 @@ int sht_get_option(const sht_plan *p, int option, int *value)
   if (!value) { set_error("NULL output"); return SHT_ERR_INVALID_ARG; }
   switch (option) {
   case SHT_OPT_LEGENDRE_KERNEL: *value = p->leg_kernel; return SHT_OK;
+  case SHT_OPT_HOST_GRAPHS: *value = p->host_graphs ? 1 : 0; return SHT_OK;
+  case SHT_OPT_HOST_GRAPH_COUNT: {
+    std::lock_guard<std::mutex> lk(const_cast<sht_plan *>(p)->mtx);
+    int n = 0;
+    for (const HostGraph &g : p->graphs) n += g.exec != nullptr;
+    *value = n;
+    return SHT_OK;
+  }
   default: set_error("unknown option"); return SHT_ERR_INVALID_ARG;
   }
 }
@@ -922,6 +1077,7 @@ static int diffuse_impl(sht_plan *p, double *w, int nb, const double *coef, doub
   if (!host) return launch_diffuse(p, w, nb, coef, dt, filter, s);
   const size_t nw = (size_t)nb * p->L, need = sizeof(double) * (nw + 2 * p->L) + 1024;
   if (need > p->io_bytes) {
+    ++p->buf_gen;
     if (p->d_io) { cudaStreamSynchronize(s); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
     if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
     p->io_bytes = need;

@@ -471,30 +471,8 @@ __global__ void __launch_bounds__(256) k_zonal_inv(FftArgs a)
 namespace {
 constexpr int kFftThreads = 128;
 
-// Persistent grid: as many blocks as fit on the device at once, never more
-// than there are tiles.  The occupancy query runs once per kernel instance and
-// buffer size.
-template <typename K>
-int persistent_blocks(K kern, size_t smem, const sht_plan *p, long long ntiles)
-{
-  struct Entry { const void *k; size_t smem; int occ; };
-  static std::mutex mu;
-  static std::vector<Entry> cache;
-  int occ = 0;
-  {
-    std::lock_guard<std::mutex> lk(mu);
-    for (const Entry &c : cache)
-      if (c.k == (const void *)kern && c.smem == smem) occ = c.occ;
-  }
-  if (occ == 0) {
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kFftThreads, smem) != cudaSuccess || occ < 1) occ = 1;
-    std::lock_guard<std::mutex> lk(mu);
-    cache.push_back({(const void *)kern, smem, occ});
-  }
-  const long long g = (long long)occ * (p->num_sms > 0 ? p->num_sms : 1);
-  return (int)(ntiles < g ? ntiles : g);
-}
-
+// Persistent grids: as many blocks as fit on the device at once, never more
+// than there are tiles.
 template <int A, int B>
 int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
 {
@@ -508,9 +486,10 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
   if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
   cudaError_t e = cudaSuccess;
   auto go = [&](auto kern, auto... extra) {
-    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return;
-    kern<<<persistent_blocks(kern, smem, p, ntiles), kFftThreads, smem, s>>>(a, extra...);
+    int occ = 0;
+    if ((e = kernel_setup((const void *)kern, smem, kFftThreads, &occ)) != cudaSuccess) return;
+    const long long g = (long long)(occ < 1 ? 1 : occ) * (p->num_sms > 0 ? p->num_sms : 1);
+    kern<<<(int)(ntiles < g ? ntiles : g), kFftThreads, smem, s>>>(a, extra...);
   };
   if (inverse) go(k_fft_inv<A, B, kFftThreads>, bufe);
   else if (a.mul) go(k_fft_fwd<A, B, kFftThreads, 1>);

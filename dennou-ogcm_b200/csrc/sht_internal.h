@@ -59,6 +59,18 @@ struct Timing {
   float ms_fft = 0.f, ms_leg = 0.f, ms_spec = 0.f;
 };
 
+// A host-pointer call staged through the plan's page-locked buffer, kept as
+// an instantiated CUDA graph (copy in, the operator's kernels, copy out).
+// Every pointer in it is a plan buffer, so it replays for any caller arrays
+// of the same operator and size until a buffer is reallocated (buf_gen).
+struct HostGraph {
+  int op = -1, nb = 0, precision = 0, leg_kernel = 0;
+  unsigned long long gen = 0;
+  cudaGraphExec_t exec = nullptr;  // null after the first call, or when not capturable
+  bool failed = false;             // capture was refused: run this call uncaptured
+  int launches = 0;                // kernels in the graph
+};
+
 }  // namespace sht
 
 struct sht_plan_s {
@@ -112,6 +124,14 @@ struct sht_plan_s {
   // split-precision tables (built lazily)
   void *tc_tables = nullptr;
 
+  // graphs of staged host-pointer calls (SHT_OPT_HOST_GRAPHS), the stream
+  // they are captured on, and the generation of the buffers they name
+  // (bumped whenever d_ws, d_io or h_stage is reallocated)
+  bool host_graphs = true;
+  std::vector<sht::HostGraph> graphs;
+  cudaStream_t cap_stream = nullptr;
+  unsigned long long buf_gen = 0;
+
   std::mutex mtx;
   sht::Timing timing;
 };
@@ -123,6 +143,12 @@ constexpr uint32_t kPlanMagic = 0x53485442u;  // "SHTB"
 void set_error(const std::string &msg);
 int cuda_fail(cudaError_t e, const char *what);
 void count_launch(int n = 1);
+
+// Dynamic shared-memory opt-in of a kernel and its resident blocks per SM at
+// (smem, threads), on the current device.  The runtime calls behind them
+// cost microseconds each, which a per-level call would pay on every launch,
+// so the results are cached per device and kernel; the opt-in only grows.
+cudaError_t kernel_setup(const void *kern, size_t smem, int threads, int *per_sm = nullptr);
 
 // --- setup kernels (sht_setup.cu)
 int build_tables(sht_plan *p);

@@ -320,8 +320,7 @@ template <typename K>
 int launch(K kern, dim3 grid, size_t smem, cudaStream_t s, const LegArgs &args, const char *name)
 {
   cudaError_t e;
-  if (smem > 48 * 1024 && (e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)) != cudaSuccess)
-    return cuda_fail(e, name);
+  if ((e = kernel_setup((const void *)kern, smem, kThreads)) != cudaSuccess) return cuda_fail(e, name);
   kern<<<grid, kThreads, smem, s>>>(args);
   count_launch();
   e = cudaGetLastError();

@@ -695,7 +695,7 @@ int launch_split(sht_plan *p, bool inverse, const double2 *in, int ncol, double2
   const int grid = (a.nitems + a.per_cta - 1) / a.per_cta;
   const size_t smem = split_smem(a.npad_max, inverse && a.seg_inv == kSegInv);
   auto kern = inverse ? k_leg_split<true> : k_leg_split<false>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = kernel_setup((const void *)kern, smem, kThreads);
   if (e != cudaSuccess) return cuda_fail(e, "split smem attribute");
   kern<<<grid, kThreads, smem, s>>>(a);
   count_launch();

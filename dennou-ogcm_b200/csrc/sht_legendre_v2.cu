@@ -388,10 +388,8 @@ int launch_pair(const sht_plan *p, bool inverse, const double2 *in, int ncol, do
   case 64: kern = inverse ? k_leg_inv_pair<64> : k_leg_fwd_pair<64>; break;
   default: set_error("legendre: latitude count outside the paired kernels"); return SHT_ERR_UNSUPPORTED_SIZE;
   }
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, "legendre pair smem attribute");
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, smem);
+  cudaError_t e = kernel_setup((const void *)kern, smem, kT, &per_sm);
   if (e != cudaSuccess || per_sm < 1) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidConfiguration : e, "legendre pair occupancy");
   const int slots = p->num_sms * per_sm;
   a.per_cta = (a.nitems + slots - 1) / slots;

@@ -389,10 +389,8 @@ bool choose(const sht_plan *p, Choice *c)
 template <typename K>
 int run(K kern, size_t smem, const sht_plan *p, V3Args &a, cudaStream_t s, const char *name)
 {
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (e != cudaSuccess) return cuda_fail(e, "legendre chunked smem attribute");
   int per_sm = 0;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kT, smem);
+  cudaError_t e = kernel_setup((const void *)kern, smem, kT, &per_sm);
   if (e != cudaSuccess || per_sm < 1) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidConfiguration : e, name);
   const int slots = p->num_sms * per_sm;
   a.per_cta = (a.nitems + slots - 1) / slots;

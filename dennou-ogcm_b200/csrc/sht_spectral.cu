@@ -355,7 +355,7 @@ int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1,
   cudaError_t e = cudaSuccess;
   auto run = [&](auto kern, int nslots) {
     const size_t smem = one * nslots;
-    if (smem > 48 * 1024) e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    e = kernel_setup((const void *)kern, smem, 256);
     if (e == cudaSuccess) kern<<<grid, 256, smem, s>>>(a);
   };
   switch (op) {

@@ -30,6 +30,8 @@ SHT_OK = 0
 SHT_PREC_FP64 = 0
 SHT_PREC_SPLIT = 1
 SHT_OPT_LEGENDRE_KERNEL = 1
+SHT_OPT_HOST_GRAPHS = 2
+SHT_OPT_HOST_GRAPH_COUNT = 3
 SHT_MULTI_SYNTHESIS, SHT_MULTI_ANALYSIS, SHT_MULTI_ROUND_TRIP = 1, 2, 3
 SHT_MULTI_AUTOTUNE, SHT_MULTI_ALLOW_SPLIT, SHT_MULTI_NO_GRAPH = 1, 2, 4
 

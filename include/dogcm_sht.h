@@ -119,6 +119,13 @@ SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
  * latitude-chunked paired-band kernel (jm/2 a multiple of 16, up to T341).
  * A choice that does not cover the grid falls back to the automatic one. */
 #define SHT_OPT_LEGENDRE_KERNEL 1
+/* SHT_OPT_HOST_GRAPHS: 1 (default) replays small host-pointer calls (those
+ * staged through the plan's page-locked buffer) as CUDA graphs from the
+ * second call of an operator and size on; 0 launches every call directly.
+ * Either way the results are identical.  SHT_OPT_HOST_GRAPH_COUNT (read only)
+ * is the number of graphs the plan holds. */
+#define SHT_OPT_HOST_GRAPHS 2
+#define SHT_OPT_HOST_GRAPH_COUNT 3
 SHT_API int sht_set_option(sht_plan *plan, int option, int value);
 SHT_API int sht_get_option(const sht_plan *plan, int option, int *value);
 
