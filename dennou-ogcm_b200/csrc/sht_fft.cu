@@ -252,7 +252,10 @@ __device__ __forceinline__ void fwd_tile(const FftArgs &a, double2 (&v)[1 << A],
 // straight into registers; the block's one shared buffer takes the transpose
 // and the output staging.  Staging the tile with cp.async as well, in a
 // second pair of buffers, cost blocks per SM and measured the same at T85 and
-// 7-18 % slower at T170/T341.
+// 7-18 % slower at T170/T341.  Up to 16-point first passes the plain
+// transform also holds the block's next tile in registers while it works on
+// this one (3 instead of 4 blocks per SM at T85; forward 53 -> 52 us at T85,
+// 0.314 -> 0.283 ms at T170, the same at T42).
 // MUL: 0 plain, 1 product with the factor grid (FftArgs::mul), read the same way.
 template <int A, int B, int NT, int MUL>
 __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
@@ -269,24 +272,69 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
   const int ntile = (a.JH + JTh - 1) / JTh;
   const long long ntot = (long long)a.ncol * ntile;
   const long long IJ = (long long)a.I * a.J;
-  for (long long t = blockIdx.x; t < ntot; t += gridDim.x) {
-    const int c2 = (int)(t / ntile), h0 = (int)(t - (long long)c2 * ntile) * JTh;
-    const int col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
-    const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
-    const bool valid = jh < a.JH;
+  // tile t -> (column, first row pair); this thread's row j and whether it exists
+  auto where = [&](long long t, int &col, int &h0, int &j, bool &valid) {
+    const int c2 = (int)(t / ntile);
+    h0 = (int)(t - (long long)c2 * ntile) * JTh;
+    col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
+    const int jh = h0 + (r % JTh);
+    j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
+    valid = jh < a.JH;
+  };
+  auto row_src = [&](int col, int j, bool valid) {
     const double *gb = a.gcol ? a.gcol[col]
                      : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
-    const double2 *src = reinterpret_cast<const double2 *>(gb) + (long long)(valid ? j : 0) * NC;
+    return reinterpret_cast<const double2 *>(gb) + (long long)(valid ? j : 0) * NC;
+  };
+  if (MUL == 0 && A <= 4) {
+    // The rows of the block's next tile are loaded into registers before
+    // this tile is transformed, so their DRAM latency overlaps the DFTs
+    // (not at 32-point first passes, where the second set would spill).
+    long long t = blockIdx.x;
+    double2 v[R1];
+    if (t < ntot) {
+      int col, h0, j; bool valid;
+      where(t, col, h0, j, valid);
+      const double2 *src = row_src(col, j, valid);
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? __ldcs(src + R2 * n1 + u) : make_double2(0.0, 0.0);
+    }
+    for (; t < ntot; t += gridDim.x) {
+      double2 vn[R1];
+      const long long tn = t + gridDim.x;
+      if (tn < ntot) {
+        int coln, h0n, jn; bool validn;
+        where(tn, coln, h0n, jn, validn);
+        const double2 *src = row_src(coln, jn, validn);
+#pragma unroll
+        for (int n1 = 0; n1 < R1; ++n1) vn[n1] = validn ? __ldcs(src + R2 * n1 + u) : make_double2(0.0, 0.0);
+      }
+      int col, h0, j; bool valid;
+      where(t, col, h0, j, valid);
+      fwd_tile<A, B, NT>(a, v, cur, stw, stwI, col, h0, j, valid);
+      __syncthreads();  // the output runs are read; the next tile reuses the buffer
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) v[n1] = vn[n1];
+    }
+    return;
+  }
+  for (long long t = blockIdx.x; t < ntot; t += gridDim.x) {
+    int col, h0, j; bool valid;
+    where(t, col, h0, j, valid);
+    const double2 *src = row_src(col, j, valid);
     double2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) v[n1] = valid ? __ldcs(src + R2 * n1 + u) : make_double2(0.0, 0.0);
-    if (MUL == 1) {
-      const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)(valid ? j : 0) * NC;
+    if (MUL == 0) {
+      fwd_tile<A, B, NT>(a, v, cur, stw, stwI, col, h0, j, valid);
+      __syncthreads();
+      continue;
+    }
+    const double2 *frow = reinterpret_cast<const double2 *>(a.mul + (long long)(col % a.nmul) * IJ) + (long long)(valid ? j : 0) * NC;
 #pragma unroll
-      for (int n1 = 0; n1 < R1; ++n1) {
-        const double2 q = valid ? __ldg(frow + R2 * n1 + u) : make_double2(0.0, 0.0);
-        v[n1] = make_double2(v[n1].x * q.x, v[n1].y * q.y);
-      }
+    for (int n1 = 0; n1 < R1; ++n1) {
+      const double2 q = valid ? __ldg(frow + R2 * n1 + u) : make_double2(0.0, 0.0);
+      v[n1] = make_double2(v[n1].x * q.x, v[n1].y * q.y);
     }
     fwd_tile<A, B, NT>(a, v, cur, stw, stwI, col, h0, j, valid);
     __syncthreads();  // the output runs are read; the next tile reuses the buffer
