@@ -83,7 +83,8 @@ def _rel(a, b):
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
     """Samples SM clock, max clock, power and clock-event reasons through NVML
-    every 5 ms in a background thread while the timed region runs."""
+    every millisecond in a background thread while the timed region runs (a
+    few milliseconds at the default step count)."""
 
     REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
                ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
@@ -128,7 +129,7 @@ class ClockSampler:
                             self.reasons.add(name)
                 except Exception as ex:
                     self.err = str(ex)
-                self._stop.wait(0.005)
+                self._stop.wait(0.001)
 
         self._thr = threading.Thread(target=run, daemon=True)
         self._thr.start()
