@@ -937,6 +937,18 @@ int sht_get_option(const sht_plan *p, int option, int *value)
   }
 }
 
+int sht_selftest_device_timeout(sht_plan *p, int limit_ms)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (limit_ms < 1 || limit_ms > 1000) { set_error("limit_ms must be in 1..1000"); return SHT_ERR_INVALID_ARG; }
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
+  if ((rc = wait_selftest(p, (unsigned long long)limit_ms * 1000000ull))) return rc;
+  return device_error_status(p);
+}
+
 int sht_set_stream(sht_plan *p, void *stream)
 {
   int rc = check_plan(p);

@@ -187,6 +187,8 @@ int launch_leg_inv_split(sht_plan *p, const double2 *S, int ncol, double2 *F, cu
 void free_split_tables(sht_plan *p);
 bool split_supported(const sht_plan *p);
 int split_error_status(sht_plan *p);  // reads and clears the device error word (synchronous)
+// one block whose bounded wait runs out on purpose and sets the error word (synchronous)
+int wait_selftest(sht_plan *p, unsigned long long limit_ns);
 // Reads and clears every device error word of the plan (synchronous).
 int device_error_status(sht_plan *p);
 

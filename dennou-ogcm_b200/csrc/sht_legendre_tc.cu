@@ -725,6 +725,39 @@ int launch_leg_inv_split(sht_plan *p, const double2 *Sp, int ncol, double2 *F, c
   return launch_split(p, true, Sp, ncol, F, s);
 }
 
+// The failure path of the bounded waits, run on purpose: one block waits on a
+// shared-memory barrier that nothing arrives at, through the same
+// tc::mbar_wait the split kernel uses, gives up after limit_ns and records the
+// timeout in the plan's error word as the split kernel does.  It holds no
+// TMEM and waits on nothing outside its own block.
+__global__ void __launch_bounds__(128) k_wait_selftest(int *err, unsigned long long limit_ns)
+{
+  __shared__ __align__(8) uint64_t mbar;
+  if (threadIdx.x == 0) {
+    tc::mbar_init(&mbar, 1);
+    tc::mbar_fence_init();
+  }
+  __syncthreads();
+  const bool done = tc::mbar_wait(&mbar, 0, limit_ns);
+  if (!done && (threadIdx.x & 31) == 0) atomicExch(err, SHT_ERR_DEVICE_TIMEOUT);
+  __syncthreads();
+}
+
+int wait_selftest(sht_plan *p, unsigned long long limit_ns)
+{
+  if (!split_supported(p)) {
+    set_error("device timeout self-test: this grid has no split-precision error word");
+    return SHT_ERR_UNSUPPORTED_SIZE;
+  }
+  int rc = build_split_tables(p);
+  if (rc) return rc;
+  k_wait_selftest<<<1, 128, 0, p->stream>>>(tables(p)->d_err, limit_ns);
+  count_launch();
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaStreamSynchronize(p->stream);
+  return e == cudaSuccess ? SHT_OK : cuda_fail(e, "k_wait_selftest");
+}
+
 int split_error_status(sht_plan *p)
 {
   SplitTables *t = tables(p);

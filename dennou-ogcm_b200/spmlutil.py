@@ -84,6 +84,7 @@ def load_library(path: str | None = None):
     lib.sht_set_option.argtypes = [_VP, ctypes.c_int, ctypes.c_int]
     lib.sht_get_option.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.sht_synchronize.argtypes = [_VP]
+    lib.sht_selftest_device_timeout.argtypes = [_VP, ctypes.c_int]
     lib.sht_set_timing.argtypes = [_VP, ctypes.c_int]
     lib.sht_last_timing.argtypes = [_VP] + [ctypes.POINTER(ctypes.c_float)] * 3
     lib.sht_launch_count.restype = ctypes.c_longlong

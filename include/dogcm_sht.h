@@ -129,6 +129,17 @@ SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
 SHT_API int sht_set_option(sht_plan *plan, int option, int value);
 SHT_API int sht_get_option(const sht_plan *plan, int option, int *value);
 
+/* Self-test of the device-side failure path: one block waits, through the
+ * bounded wait the split-precision kernel uses, on a shared-memory barrier
+ * that nothing arrives at, gives up after limit_ms milliseconds (1..1000)
+ * and records the timeout in the plan's device error word.  Returns what the
+ * status check after a synchronous call then reports:
+ * SHT_ERR_DEVICE_TIMEOUT when the bound and the error word work.  The word is
+ * cleared and the plan stays usable.  No counterpart in the reference (its
+ * failures abort through MessageNotify).  Grids outside the split kernel
+ * return SHT_ERR_UNSUPPORTED_SIZE. */
+SHT_API int sht_selftest_device_timeout(sht_plan *plan, int limit_ms);
+
 /* Stream for the *_dev calls (a cudaStream_t passed as void*; NULL = legacy
  * default stream), and a wait for all work on it. */
 SHT_API int sht_set_stream(sht_plan *plan, void *stream);

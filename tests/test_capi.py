@@ -100,6 +100,7 @@ def test_strided_calls_check_arguments_on_the_host():
     assert lib.sht_analysis_dev(None, ptr, 66, 34, 1, ptr, 500, 1) == 3
     assert lib.sht_synthesis(None, ptr, 500, 1, ptr, 66, 34, 0) == 3
     assert lib.sht_synthesis_dev(None, ptr, 500, 0, ptr, 66, 34, -1) == 3
+    assert lib.sht_selftest_device_timeout(None, 10) == 3
 
 
 def test_init_without_device_reports_no_device(cuda_available):
