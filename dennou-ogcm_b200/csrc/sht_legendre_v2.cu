@@ -14,7 +14,10 @@
 // fragment load touches 16 distinct double-word bank pairs:
 //   P rows (stride-2 rows of one parity):  PS = 2 (mod 8) doubles (synthesis,
 //     8-byte fragment loads), 4 (mod 8) (analysis, 16-byte fragment loads)
-//   data rows (columns of one panel):      CS = 8 (mod 16) doubles
+//   data rows (columns of one panel):      CS = 2 (mod 4) doubles: a lane's
+//     16-byte B load sits at chunk (row CS/2 + 2q) mod 8 of its row pair, and an
+//     odd CS/2 puts the two rows of a quarter-warp on the odd and even chunks
+//     (CS = 8 (mod 16) put both on the even ones: a 2-way conflict per load)
 //   coefficient rows (stride-2 rows):      AS = 2 (mod 8) doubles
 // Used when a pair's P rows and the data panels fit in shared memory (T85 and
 // smaller); larger grids use the chunked kernels of sht_legendre_v3.cu.
@@ -54,7 +57,7 @@ __host__ __device__ inline Geo make_geo(int N, int J, bool analysis)
   Geo g;
   const int JH = J / 2;
   g.PS = round_mod(JH, analysis ? 4 : 2, 8);
-  g.CS = round_mod(2 * J, 8, 16);
+  g.CS = round_mod(2 * J, 2, 4);
   g.AS = round_mod(2 * kCT, 2, 8);
   g.prow_cap = N + 4;
   g.arow_cap = (N + 2 + 8 + 7) & ~7;  // rows of the larger band plus a zeroed tail (a k-step reads up to 7 rows past it)
