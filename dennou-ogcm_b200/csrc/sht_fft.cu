@@ -21,6 +21,7 @@
 // Shared-memory strides are padded so that each 8-lane phase of a 16-byte
 // access touches eight distinct bank groups.
 #include "sht_internal.h"
+#include "sht_l2.cuh"
 
 namespace sht {
 
@@ -234,15 +235,17 @@ __device__ __forceinline__ void fwd_tile(const FftArgs &a, double2 (&v)[1 << A],
   }
   __syncthreads();
 
-  // runs Gs = north + south at F[m][col][jh], Ga = north - south at F[m][col][JH + jh]
+  // runs Gs = north + south at F[m][col][jh], Ga = north - south at F[m][col][JH + jh],
+  // kept in L2 for the Legendre contraction that reads them next
   const int nh = min(JTh, a.JH - h0);
   double2 *Fb = a.F + (long long)(a.colF0 + col) * a.J + h0;
+  const uint64_t keep = l2::keep_policy();
   for (int idx = tid; idx < (a.N + 1) * JTh; idx += NT) {
     const int m = idx / JTh, i = idx - m * JTh;
     if (i < nh) {
       const double2 gn = cur[m * JTp + i], gs = cur[m * JTp + JTh + i];
-      Fb[m * mstride + i] = make_double2(gn.x + gs.x, gn.y + gs.y);
-      Fb[m * mstride + a.JH + i] = make_double2(gn.x - gs.x, gn.y - gs.y);
+      l2::st_keep(Fb + m * mstride + i, make_double2(gn.x + gs.x, gn.y + gs.y), keep);
+      l2::st_keep(Fb + m * mstride + a.JH + i, make_double2(gn.x - gs.x, gn.y - gs.y), keep);
     }
   }
 }
@@ -442,6 +445,20 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
       v[n1] = make_double2((X.x + Y.x) - ti, (X.y + Y.y) + tr);
     }
     __syncthreads();  // the staged runs are consumed; the buffer is reused below
+    if constexpr (JTh * 16 % 128 == 0) {
+      // Each E and O run of this tile is a whole number of 128-byte lines
+      // (when JH is a multiple of the run) that no later kernel reads: drop
+      // them from L2 without a write-back.
+      if (a.JH % JTh == 0) {
+        constexpr int LPR = JTh * 16 / 128;
+        const double2 *Fb = a.Fc + (long long)(a.colF0 + col) * a.J + h0;
+        for (int q = tid; q < (a.N + 1) * 2 * LPR; q += NT) {
+          const int m = q / (2 * LPR), rest = q - m * 2 * LPR;
+          l2::discard_line(reinterpret_cast<const char *>(Fb + m * mstride + (rest < LPR ? 0 : a.JH)) +
+                           128 * (rest % LPR));
+        }
+      }
+    }
 
     dft_reg<A, true>(v);
     double2 *srow = cur + r * RS;

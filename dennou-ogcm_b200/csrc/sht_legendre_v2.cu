@@ -28,6 +28,7 @@
 // F[m][col][jh] and F[m][col][JH + jh].
 #include "sht_internal.h"
 #include "sht_dmma.cuh"
+#include "sht_l2.cuh"
 
 namespace sht {
 
@@ -145,6 +146,19 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
     cp_wait0();
     __syncthreads();
     double *const Gcur = G0;  // column rows: Gs at [0, JH), Ga at [JH, J)
+    {
+      // The panel's Fourier lines are in shared memory now and no later kernel
+      // reads them: drop them from L2 without a write-back.  A column row is
+      // J complex values, a whole number of 128-byte lines.
+      constexpr int CT = ct_fwd(JH), LPR = 2 * JH * 16 / 128;
+      const int nrow = (pr.y >= 0) ? 2 * CT : CT;
+      for (int q = threadIdx.x; q < nrow * LPR; q += kT) {
+        const int row = q / LPR, b = row % CT, m = (row / CT) ? pr.y : pr.x;
+        if (col0 + b < a.ncol)
+          l2::discard_line(reinterpret_cast<const char *>(a.F + ((long long)m * a.ncol + col0 + b) * (2 * JH)) +
+                           128 * (q % LPR));
+      }
+    }
 
     // jobs: (band, parity, 16-row group)
     const int Ra = a.N + 2 - pr.x, Rb = (pr.y >= 0) ? a.N + 2 - pr.y : 0;
@@ -254,6 +268,7 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
   constexpr int ngrp = kW / ntj;          // 4, 2 or 1
   constexpr int nnt = 4 / ngrp;           // column tiles (of 8 reals) per unit
   const int jt = warp % ntj, grp = warp / ntj;
+  const uint64_t keep = l2::keep_policy();  // the Fourier runs stay in L2 for the longitude transform
 
   {
     const int2 pr = a.pairs[it0 / a.ntiles];
@@ -320,8 +335,8 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
             const int c = col0 + cb + 8 * u2 + 2 * (lane & 3) + e;
             if (c >= a.ncol) continue;
             double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
-            Fc[jh] = make_double2(acc[0][2 * u2][e], acc[0][2 * u2 + 1][e]);       // even degrees
-            Fc[JH + jh] = make_double2(acc[1][2 * u2][e], acc[1][2 * u2 + 1][e]);  // odd degrees
+            l2::st_keep(Fc + jh, make_double2(acc[0][2 * u2][e], acc[0][2 * u2 + 1][e]), keep);       // even degrees
+            l2::st_keep(Fc + JH + jh, make_double2(acc[1][2 * u2][e], acc[1][2 * u2 + 1][e]), keep);  // odd degrees
           }
       } else {
         for (int t0 = 0; t0 < kp; t0 += 4) {
@@ -342,8 +357,8 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
           const int c = col0 + 4 * (grp * nnt + q) + (lane & 3);
           if (c >= a.ncol) continue;
           double2 *Fc = a.Fo + ((long long)m * a.ncol + c) * (2 * JH);
-          Fc[jh] = make_double2(acc[0][q][0], acc[0][q][1]);       // even degrees
-          Fc[JH + jh] = make_double2(acc[1][q][0], acc[1][q][1]);  // odd degrees
+          l2::st_keep(Fc + jh, make_double2(acc[0][q][0], acc[0][q][1]), keep);       // even degrees
+          l2::st_keep(Fc + JH + jh, make_double2(acc[1][q][0], acc[1][q][1]), keep);  // odd degrees
         }
       }
     }
