@@ -548,6 +548,13 @@ def main():
                 / float(peaks.get("hbm_gbs", 6650.0)),
                 "legendre_frac_of_fp64": (2 * leg_flops / ((st["syn"][1] + st["ana"][1]) * 1e-3) / 1e12)
                 / max(fp64_dmma.value, 1e-9)}
+    # whole step against the fused round-trip floor: a round trip that read
+    # and wrote each grid and each spectrum once, 2 (8 I J + 8 (N+1)^2) bytes
+    # per field-level, at the measured HBM bandwidth
+    floor_b = 2 * (8 * I * J + 8 * (N + 1) ** 2) * nb
+    roofline["round_trip_floor"] = {
+        "bytes_per_step": floor_b, "achieved_gbs": floor_b / (head["ms_per_step"] * 1e-3) / 1e9,
+        "frac_of_hbm": floor_b / (head["ms_per_step"] * 1e-3) / 1e9 / float(peaks.get("hbm_gbs", 6650.0))}
 
     # e2e through the host-pointer C-ABI
     e2e = None
