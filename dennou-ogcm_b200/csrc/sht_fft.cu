@@ -374,14 +374,23 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
     }
   };
 
+  // Up to 16-point first passes the next tile's runs stream into the second
+  // buffer while this one is transformed.  At 32 points a buffer is 67 KB and
+  // the kernel needs 254 registers: one buffer per block, so that two blocks
+  // share an SM and one block's loads overlap the other's transform.
+  constexpr bool kDB = A <= 4;
   long long t = blockIdx.x;
   if (t < ntot) issue(t, sm);
   cp_async_commit();
   for (int it = 0; t < ntot; t += gridDim.x, ++it) {
-    double2 *cur = sm + (it & 1) * bufe;
-    if (t + gridDim.x < ntot) issue(t + gridDim.x, sm + ((it + 1) & 1) * bufe);
-    cp_async_commit();
-    cp_async_wait<1>();
+    double2 *cur = kDB ? sm + (it & 1) * bufe : sm;
+    if constexpr (kDB) {
+      if (t + gridDim.x < ntot) issue(t + gridDim.x, sm + ((it + 1) & 1) * bufe);
+      cp_async_commit();
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
     __syncthreads();
 
     const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
@@ -493,6 +502,10 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
         }
     }
     __syncthreads();  // the buffer is refilled by the prefetch of the next iteration
+    if constexpr (!kDB) {
+      if (t + gridDim.x < ntot) issue(t + gridDim.x, sm);
+      cp_async_commit();
+    }
   }
   cp_async_wait<0>();
 }
@@ -542,10 +555,10 @@ template <int A, int B>
 int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
 {
   using S = FftShape<A, B, kFftThreads>;
-  // inverse: two buffers (staged Fourier runs of the next tile beside the
-  // current one); forward: one buffer
+  // inverse up to 16-point first passes: two buffers (staged Fourier runs of
+  // the next tile beside the current one); otherwise one buffer
   const int bufe = S::buf_elems(p->N);
-  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + (inverse ? 2 : 1) * (size_t)bufe);
+  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + (inverse && A <= 4 ? 2 : 1) * (size_t)bufe);
   const long long ntiles = (long long)a.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
   if (ntiles <= 0) return SHT_OK;
   if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
