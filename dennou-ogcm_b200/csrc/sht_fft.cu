@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
 // Inverse transform, persistent over tiles; the Fourier runs of tile
 // t+gridDim.x stream into one buffer while tile t is transformed in place.
 template <int A, int B, int NT>
-__global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
+__global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftArgs a, int bufe)
 {
   using S = FftShape<A, B, NT>;
   constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT, RS = S::RS, JTp = S::JTp;
@@ -377,8 +377,10 @@ __global__ void __launch_bounds__(NT) k_fft_inv(FftArgs a, int bufe)
   // Up to 16-point first passes the next tile's runs stream into the second
   // buffer while this one is transformed.  At 32 points a buffer is 67 KB and
   // the kernel needs 254 registers: one buffer per block, so that two blocks
-  // share an SM and one block's loads overlap the other's transform.
-  constexpr bool kDB = A <= 4;
+  // share an SM and one block's loads overlap the other's transform.  At 128
+  // complex points (I = 256) one buffer and a 128-register cap give 4 blocks
+  // per SM instead of 3 (inverse 55.0 -> 53.9 us at T85, 480 field-levels).
+  constexpr bool kDB = A <= 4 && !(A == 4 && B == 3);
   long long t = blockIdx.x;
   if (t < ntot) issue(t, sm);
   cp_async_commit();
@@ -558,7 +560,7 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
   // inverse up to 16-point first passes: two buffers (staged Fourier runs of
   // the next tile beside the current one); otherwise one buffer
   const int bufe = S::buf_elems(p->N);
-  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + (inverse && A <= 4 ? 2 : 1) * (size_t)bufe);
+  const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + (inverse && A <= 4 && !(A == 4 && B == 3) ? 2 : 1) * (size_t)bufe);
   const long long ntiles = (long long)a.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
   if (ntiles <= 0) return SHT_OK;
   if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
