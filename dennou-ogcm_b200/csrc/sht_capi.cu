@@ -140,6 +140,24 @@ int ensure_ws(sht_plan *p, int ncol, int nb_temp, Workspace *ws)
   return SHT_OK;
 }
 
+// The device staging of the host-pointer calls, grown on demand (a growth
+// invalidates the plan's host-call graphs, which name the old array).
+int ensure_io(sht_plan *p, size_t need)
+{
+  if (need <= p->io_bytes) return SHT_OK;
+  ++p->buf_gen;
+  if (p->d_io) {
+    cudaStreamSynchronize(p->stream);
+    cudaFree(p->d_io);
+    p->d_io = nullptr;
+    p->io_bytes = 0;
+  }
+  cudaError_t e = cudaMalloc(&p->d_io, need);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
+  p->io_bytes = need;
+  return SHT_OK;
+}
+
 void mark(sht_plan *p, int k, cudaStream_t s)
 {
   if (p->timing.on) cudaEventRecord(p->timing.ev[k], s);
@@ -457,12 +475,7 @@ int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, d
   auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };  // in doubles
   const size_t need = sizeof(double) * (al(nin_each) * sh.nin + al(nout_each) * sh.nout) + 1024;
   cudaError_t e;
-  if (need > p->io_bytes) {
-    ++p->buf_gen;
-    if (p->d_io) { cudaStreamSynchronize(p->stream); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
-    if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
-    p->io_bytes = need;
-  }
+  if ((rc = ensure_io(p, need))) return rc;
   double *d = static_cast<double *>(p->d_io);
   // staging: the operator's inputs, then its outputs
   const double *hin[3] = {i0, i1, i2};
@@ -653,14 +666,8 @@ int strided_staging(sht_plan *p, int nb, double **dg, double **dw)
 {
   auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };
   const size_t ng = (size_t)nb * p->I * p->J, nw = (size_t)nb * p->L;
-  const size_t need = sizeof(double) * (al(ng) + al(nw)) + 1024;
-  if (need > p->io_bytes) {
-    cudaError_t e;
-    ++p->buf_gen;
-    if (p->d_io) { cudaStreamSynchronize(p->stream); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
-    if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
-    p->io_bytes = need;
-  }
+  const int rc = ensure_io(p, sizeof(double) * (al(ng) + al(nw)) + 1024);
+  if (rc) return rc;
   *dg = static_cast<double *>(p->d_io);
   *dw = *dg + al(ng);
   return SHT_OK;
@@ -963,6 +970,7 @@ int sht_synchronize(sht_plan *p)
   int rc = check_plan(p);
   if (rc) return rc;
   DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
   cudaError_t e = cudaStreamSynchronize(p->stream);
   if (e != cudaSuccess) return cuda_fail(e, "synchronize");
   return device_error_status(p);
@@ -1084,16 +1092,12 @@ static int diffuse_impl(sht_plan *p, double *w, int nb, const double *coef, doub
   if (nb == 0) return SHT_OK;
   std::lock_guard<std::mutex> lk(p->mtx);
   DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
   cudaStream_t s = p->stream;
   cudaError_t e;
   if (!host) return launch_diffuse(p, w, nb, coef, dt, filter, s);
-  const size_t nw = (size_t)nb * p->L, need = sizeof(double) * (nw + 2 * p->L) + 1024;
-  if (need > p->io_bytes) {
-    ++p->buf_gen;
-    if (p->d_io) { cudaStreamSynchronize(s); cudaFree(p->d_io); p->d_io = nullptr; p->io_bytes = 0; }
-    if ((e = cudaMalloc(&p->d_io, need)) != cudaSuccess) return cuda_fail(e, "cudaMalloc(io staging)");
-    p->io_bytes = need;
-  }
+  const size_t nw = (size_t)nb * p->L;
+  if ((rc = ensure_io(p, sizeof(double) * (nw + 2 * p->L) + 1024))) return rc;
   double *dw = static_cast<double *>(p->d_io), *dc = dw + nw, *df = dc + p->L;
   if ((e = cudaMemcpyAsync(dw, w, sizeof(double) * nw, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
       (e = cudaMemcpyAsync(dc, coef, sizeof(double) * p->L, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
@@ -1119,6 +1123,7 @@ int sht_roundtrip_diffuse_dev(sht_plan *p, double *xya, int nb, const double *co
   if (nb == 0) return SHT_OK;
   std::lock_guard<std::mutex> lk(p->mtx);
   DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
   Workspace ws;
   if ((rc = ensure_ws(p, nb, nb, &ws))) return rc;
   if ((rc = run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, xya, nullptr, nb, ws.W, nullptr))) return rc;
