@@ -277,6 +277,9 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
   const long long IJ = (long long)a.I * a.J;
   // tile t -> (column, first row pair); this thread's row j and whether it exists
   auto where = [&](long long t, int &col, int &h0, int &j, bool &valid) {
+    // last column first: when a synthesis has just written the grid, its
+    // last columns are the likeliest to be still in L2
+    t = ntot - 1 - t;
     const int c2 = (int)(t / ntile);
     h0 = (int)(t - (long long)c2 * ntile) * JTh;
     col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
@@ -500,7 +503,7 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
 #pragma unroll
         for (int k2 = 0; k2 < R2; ++k2) {
           const double2 w = z[s][brev<B>(k2)];
-          __stcs(rowp + (u + T * s + R1 * k2), make_double2(w.x * sc, w.y * sc));
+          rowp[u + T * s + R1 * k2] = make_double2(w.x * sc, w.y * sc);  // default policy: may stay in L2 for an analysis
         }
     }
     __syncthreads();  // the buffer is refilled by the prefetch of the next iteration
