@@ -30,6 +30,24 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_header_is_plain_c(tmp_path):
+    """include/dogcm_sht.h is usable from C99 and C++ hosts (the Fortran shim
+    binds the same declarations through ISO_C_BINDING)."""
+    import shutil
+    import subprocess
+
+    src = tmp_path / "use_header.c"
+    src.write_text('#include "dogcm_sht.h"\n'
+                   "int main(void) { sht_plan *p = 0; return sht_wa_xya(p, 0, 0, 0) + SHT_OK; }\n")
+    inc = os.path.dirname(HEADER)
+    for cc, std in (("gcc", ["-std=c99", "-pedantic"]), ("g++", ["-std=c++11", "-x", "c++"])):
+        if shutil.which(cc) is None:
+            pytest.skip(f"{cc} not available")
+        r = subprocess.run([cc, *std, "-Wall", "-Wextra", "-Werror", "-fsyntax-only", "-I", inc, str(src)],
+                           capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+
+
 def test_fortran_shim_binds_declared_symbols():
     """Every bind(C) interface of the Fortran front end names a declared entry
     point, with as many arguments as the C declaration (no Fortran compiler
