@@ -61,8 +61,9 @@ def _peaks():
 
 def _traffic(kernel, mode, nb, grid=GRID):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
-    capture of this workload (profiles/t85_roundtrip_fp64.md), FP64 path at the
-    480 field-level batch; None for any other configuration."""
+    capture of this workload (the per-kernel dram__bytes_read.sum +
+    dram__bytes_write.sum kept in profiles/t85_dram_traffic.json), FP64 path at
+    the 480 field-level batch; None for any other configuration."""
     if mode != "fp64" or nb != LEVELS * FIELDS or grid != GRID:
         return None
     try:
@@ -188,7 +189,22 @@ def run_reference(args):
     return 0
 
 
-def cpu_baseline(nb, grid=GRID, seconds=10.0):
+def _per_field(got, ref, levels):
+    """Largest normwise relative error of each field (field f = levels
+    [f L, (f+1) L) of the batch), over its levels."""
+    got = np.asarray(got).reshape(len(got), -1)
+    ref = np.asarray(ref).reshape(len(ref), -1)
+    e = np.abs(got - ref).max(1) / np.where(np.abs(ref).max(1) == 0, 1.0, np.abs(ref).max(1))
+    return [float(e[f * levels:(f + 1) * levels].max()) for f in range(len(e) // levels)]
+
+
+def cpu_baseline(w_in, grid=GRID, seconds=10.0, checks=None, levels=LEVELS):
+    """The oracle on all host cores, timed on the benchmark's own seeded
+    spectra (a bounded sample of the same round trip), and the checker of the
+    GPU results: `checks` maps a label to (inputs, GPU synthesis grid, GPU
+    analysis of that grid[, grid name, levels]); each is compared with the
+    oracle's synthesis of the inputs and the oracle's analysis of the GPU grid,
+    field by field."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     W = importlib.import_module("dennou-ogcm_b200.workloads")
@@ -196,15 +212,31 @@ def cpu_baseline(nb, grid=GRID, seconds=10.0):
     cores = os.cpu_count() or 1
     O.set_threads(cores)
     p = O.OraclePlan(I, J, N, RADIUS)
-    w = W.seeded_spectra(N, nb, POWER)
-    p.wa_xya(p.xya_wa(w))
+    nb = len(w_in)
+    p.wa_xya(p.xya_wa(w_in))
     done, t0 = 0, time.perf_counter()
     while time.perf_counter() - t0 < seconds:
-        p.wa_xya(p.xya_wa(w))
+        p.wa_xya(p.xya_wa(w_in))
         done += nb
     el = time.perf_counter() - t0
-    return {"value": done / el, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{done} field-level round trips ({done // nb} batches of {nb}) in {el:.1f} s"}
+    out = {"value": done / el, "unit": UNIT, "cores": cores, "kind": "port",
+           "sample": f"{done} field-level round trips ({done // nb} batches of {nb}) in {el:.1f} s"}
+    if checks:
+        rel = {}
+        plans = {grid: p}
+        for label, item in checks.items():
+            w, g_gpu, w_gpu = item[:3]
+            gname, lv = (item[3], item[4]) if len(item) > 3 else (grid, levels)
+            if gname not in plans:
+                plans[gname] = O.OraclePlan(*W.GRIDS[gname], RADIUS)
+            q = plans[gname]
+            syn = _per_field(g_gpu, q.xya_wa(w), lv)
+            ana = _per_field(w_gpu, q.wa_xya(g_gpu), lv)
+            rel[label] = {"grid": gname, "field_levels": len(w), "levels_per_field": lv,
+                          "synthesis_max": max(syn), "analysis_max": max(ana),
+                          "synthesis_per_field": syn, "analysis_per_field": ana}
+        out["relerr_vs_oracle"] = rel
+    return out
 
 
 # ------------------------------------------------------------------ ours
@@ -391,6 +423,28 @@ def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
     return out
 
 
+def c2_outputs(P, W, torch, dev):
+    """Config C2 (T170, 60 levels x 12 fields, spectra ~(n+1)^-1.5) in both
+    precisions: one synthesis of the seeded spectra and one analysis of the
+    resulting grid each, for the per-field oracle check of the cpu_baseline leg."""
+    c = W.CONFIGS["C2"]
+    I, J, N = W.GRIDS[c["grid"]]
+    nb = c["levels"] * c["fields"]
+    sht = P.SpmlUtil(I, J, 1, N, None, RADIUS)
+    w = W.seeded_spectra_torch(N, nb, c["power"], dev)
+    out = {}
+    try:
+        for mode, prec in (("fp64", P.SHT_PREC_FP64), ("split", P.SHT_PREC_SPLIT)):
+            sht.set_precision(prec)
+            g = sht.xya_wa(w)
+            back = sht.wa_xya(g)
+            torch.cuda.synchronize()
+            out[f"C2_{mode}"] = (w.cpu().numpy(), g.cpu().numpy(), back.cpu().numpy(), c["grid"], c["levels"])
+    finally:
+        sht.final()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -403,6 +457,7 @@ def main():
                     help="resolution (default T85, the headline workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-c2", action="store_true", help="skip the C2 (T170 L60 x 12) per-field oracle check")
     ap.add_argument("--no-multi", action="store_true", help="skip the C3 multi-instance measurement")
     ap.add_argument("--no-fused", action="store_true", help="skip the fused-client measurements")
     ap.add_argument("--no-operators", action="store_true", help="skip the per-operator measurements")
@@ -445,6 +500,8 @@ def main():
     barrier = rep.barrier
     max_over_ranks = rep.max
 
+    outputs = {}
+
     def timed(prec):
         sht.set_precision(prec)
         for _ in range(args.warmup):
@@ -475,6 +532,7 @@ def main():
         ms = [a.elapsed_time(b) for a, b in evs]
         tot = max_over_ranks(sum(ms))
         err = _rel(w_out.cpu().numpy(), w_in.cpu().numpy())
+        outputs[prec] = (grid.cpu().numpy(), w_out.cpu().numpy())
         return {"value": world * nb * args.steps / (tot * 1e-3), "ms_per_step": tot / args.steps,
                 "launches": launches, "clocks": clocks, "relerr": err, "wall_s": wall}
 
@@ -515,8 +573,9 @@ def main():
     # roofline of the dominant kernel (largest share of the round trip)
     peaks, pk_kind = _peaks()
     fp64_dfma, fp64_dmma = ctypes.c_double(), ctypes.c_double()
-    lib.sht_probe_fp64_tflops.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
-    lib.sht_probe_fp64_tflops(ctypes.byref(fp64_dfma), ctypes.byref(fp64_dmma))
+    probe = ctypes.CDLL(os.path.join(ROOT, "dennou-ogcm_b200", "probe", "libfp64_peak.so"))
+    probe.fp64_peak_tflops.argtypes = [ctypes.POINTER(ctypes.c_double)] * 2
+    probe.fp64_peak_tflops(ctypes.byref(fp64_dfma), ctypes.byref(fp64_dmma))
     st = head["stages_ms"]
     fft_bytes = (8 * I * J + 16 * (N + 1) * J) * nb           # per launch, per direction
     leg_flops = 2 * J * (N + 1) * (N + 2) * nb                  # per launch, per direction (non-symmetric count)
@@ -587,7 +646,14 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(nb, args.grid)
+        checks = {}
+        for mode in modes:
+            prec = P.SHT_PREC_FP64 if mode == "fp64" else P.SHT_PREC_SPLIT
+            if prec in outputs:
+                checks[f"{args.grid}_{mode}"] = (w_in.cpu().numpy(), *outputs[prec])
+        if args.grid == GRID and not args.no_c2:
+            checks.update(c2_outputs(P, W, torch, dev))
+        cpu = cpu_baseline(w_in.cpu().numpy(), args.grid, checks=checks, levels=lv)
 
     if rank == 0:
         rec = {
@@ -603,6 +669,7 @@ def main():
             "split_vs_fp64": (results["split"]["value"] / results["fp64"]["value"])
             if "value" in results.get("split", {}) and "value" in results.get("fp64", {}) else None,
             "relerr": head["relerr"],
+            "relerr_vs_oracle": (cpu or {}).pop("relerr_vs_oracle", None),
             "roofline": roofline,
             "fp64_peak_tflops": {"dfma": fp64_dfma.value, "dmma": fp64_dmma.value},
             "cpu_baseline": cpu,

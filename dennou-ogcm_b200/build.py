@@ -4,6 +4,8 @@ Usage:  python dennou-ogcm_b200/build.py [--force] [--verbose]
 
 Each csrc/*.cu file is compiled to an object under _build/ (rebuilt when the
 source or a header is newer) and linked into libdogcm_sht.so next to this file.
+probe/fp64_peak.cu, the benchmark's FP64 throughput probe, is built into its
+own probe/libfp64_peak.so.
 """
 from __future__ import annotations
 
@@ -20,6 +22,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdogcm_sht.so")
+# the benchmark's FP64 throughput probe: a separate library, not part of the transform
+PROBE_SRC = os.path.join(HERE, "probe", "fp64_peak.cu")
+PROBE_LIB = os.path.join(HERE, "probe", "libfp64_peak.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + [
@@ -80,6 +85,13 @@ def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
             sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
         if r.returncode != 0:
             raise RuntimeError("link failed")
+    if force or _stale(PROBE_LIB, [PROBE_SRC]):
+        cmd = [nv, *ARCH, "-O3", "-Xcompiler", "-fPIC", "-shared", PROBE_SRC, "-o", PROBE_LIB]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if verbose or r.returncode != 0:
+            sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        if r.returncode != 0:
+            raise RuntimeError("probe build failed")
     return LIB
 
 

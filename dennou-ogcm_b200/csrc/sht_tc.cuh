@@ -42,6 +42,14 @@ __host__ __device__ constexpr uint32_t idesc_bf16_f32(int M, int N)
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
+// signed 8-bit x signed 8-bit -> S32 (kind::i8), both operands K-major:
+// D format 2 (S32) at [4,6), A and B format 1 (signed 8-bit) at [7,10) and
+// [10,13), no saturation.
+__host__ __device__ constexpr uint32_t idesc_s8_s32(int M, int N)
+{
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
 // ---------------------------------------------------------------- TMEM
 __device__ __forceinline__ void tmem_alloc(uint32_t *dst_smem, uint32_t ncols)
 {
@@ -70,6 +78,17 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
 }
 
+// D[tmem] (+)= A[smem] * B[smem]^T with 8-bit integer operands and exact
+// 32-bit integer accumulation, issued by one thread
+__device__ __forceinline__ void mma_s8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accumulate)
+{
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate));
+}
+
 // arrive on an mbarrier once all previously issued tcgen05 ops of this thread complete
 __device__ __forceinline__ void mma_commit(uint64_t *mbar)
 {
@@ -84,6 +103,20 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16])
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
+}
+// 32 lanes x 32 bits, 8 consecutive columns -> 8 registers per thread
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, uint32_t (&r)[8])
+{
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+// 32 lanes x 32 bits, 4 consecutive columns -> 4 registers per thread
+__device__ __forceinline__ void tmem_ld4(uint32_t taddr, uint32_t (&r)[4])
+{
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0,%1,%2,%3}, [%4];\n"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::); }
 
@@ -100,6 +133,42 @@ __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *mbar, uint32_t bytes)
 {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(mbar)), "r"(bytes) : "memory");
+}
+
+// Plain arrive (release at CTA scope: this thread's shared-memory stores made
+// before it are visible to the threads that wait on the phase).
+__device__ __forceinline__ void mbar_arrive(uint64_t *mbar)
+{
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(mbar)) : "memory");
+}
+
+// One poll of the phase with parity `parity` (acquire when it returns true).
+__device__ __forceinline__ bool mbar_try(uint32_t mbar_addr, uint32_t parity)
+{
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar_addr), "r"(parity)
+      : "memory");
+  return done != 0;
+}
+
+// The same with a suspend-time hint: the thread may sleep up to `hint_ns`
+// inside the call until the phase completes, instead of spinning.
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t mbar_addr, uint32_t parity, uint32_t hint_ns)
+{
+  uint32_t done;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(done)
+      : "r"(mbar_addr), "r"(parity), "r"(hint_ns)
+      : "memory");
+  return done != 0;
 }
 
 // Bulk copy global -> shared of `bytes` (a multiple of 16; both addresses

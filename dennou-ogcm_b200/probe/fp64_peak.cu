@@ -1,11 +1,12 @@
-// sht_probe.cu -- FP64 throughput probe used as the roofline denominator of
-// the FP64 Legendre contraction (the driver-measured peaks cover HBM copy
-// bandwidth and BF16 GEMM only).  Two dependency-free loops: DFMA on the
-// CUDA cores and mma.sync.m8n8k4.f64 on the FP64 tensor path, timed with
-// CUDA events on a private stream.
-#include "sht_internal.h"
+// fp64_peak.cu -- FP64 throughput probe of the current device, the roofline
+// denominator of the FP64 Legendre contraction in the benchmark (the measured
+// peaks of the GPU pool cover HBM copy bandwidth and BF16 GEMM only).  It is a
+// measurement aid loaded by bench.py, not part of the transform library.
+// Two dependency-free loops: DFMA on the CUDA cores and mma.sync.m8n8k4.f64
+// on the FP64 tensor path, timed with CUDA events on a private stream.
+#include <cuda_runtime.h>
 
-namespace sht {
+namespace {
 
 __global__ void k_probe_dfma(double *out, int iters, double a, double b)
 {
@@ -43,25 +44,24 @@ __global__ void k_probe_dmma(double *out, int iters)
   out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-}  // namespace sht
+}  // namespace
 
-using namespace sht;
-
-extern "C" SHT_API int sht_probe_fp64_tflops(double *tflops_dfma, double *tflops_dmma)
+// Best of three timed runs of each loop, in TFLOP/s; 0 or a cudaError_t code.
+extern "C" __attribute__((visibility("default"))) int fp64_peak_tflops(double *tflops_dfma, double *tflops_dmma)
 {
   int dev = 0, sms = 0;
   cudaError_t e;
-  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return cuda_fail(e, "probe");
-  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return cuda_fail(e, "probe");
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return (int)e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return (int)e;
   const int blocks = sms * 4, threads = 256, iters = 4096;
   double *out = nullptr;
   cudaStream_t s = nullptr;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  int rc = SHT_OK;
-  if ((e = cudaMalloc(&out, sizeof(double) * blocks * threads)) != cudaSuccess) return cuda_fail(e, "probe alloc");
+  int rc = 0;
+  if ((e = cudaMalloc(&out, sizeof(double) * blocks * threads)) != cudaSuccess) return (int)e;
   if ((e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking)) != cudaSuccess ||
       (e = cudaEventCreate(&e0)) != cudaSuccess || (e = cudaEventCreate(&e1)) != cudaSuccess) {
-    rc = cuda_fail(e, "probe setup");
+    rc = (int)e;
   }
   double best_f = 0.0, best_m = 0.0;
   for (int rep = 0; rep < 3 && !rc; ++rep) {
@@ -70,16 +70,14 @@ extern "C" SHT_API int sht_probe_fp64_tflops(double *tflops_dfma, double *tflops
     cudaEventRecord(e0, s);
     k_probe_dfma<<<blocks, threads, 0, s>>>(out, iters, 0.999, 1e-3);
     cudaEventRecord(e1, s);
-    count_launch(2);
-    if ((e = cudaEventSynchronize(e1)) != cudaSuccess) { rc = cuda_fail(e, "probe dfma"); break; }
+    if ((e = cudaEventSynchronize(e1)) != cudaSuccess) { rc = (int)e; break; }
     cudaEventElapsedTime(&ms, e0, e1);
     const double f1 = 2.0 * 8 * 16 * (double)iters * blocks * threads / (ms * 1e-3) / 1e12;
     k_probe_dmma<<<blocks, threads, 0, s>>>(out, iters / 4);
     cudaEventRecord(e0, s);
     k_probe_dmma<<<blocks, threads, 0, s>>>(out, iters);
     cudaEventRecord(e1, s);
-    count_launch(2);
-    if ((e = cudaEventSynchronize(e1)) != cudaSuccess) { rc = cuda_fail(e, "probe dmma"); break; }
+    if ((e = cudaEventSynchronize(e1)) != cudaSuccess) { rc = (int)e; break; }
     cudaEventElapsedTime(&ms, e0, e1);
     const double f2 = 2.0 * 256 * 8 * (double)iters * blocks * (threads / 32) / (ms * 1e-3) / 1e12;
     if (f1 > best_f) best_f = f1;

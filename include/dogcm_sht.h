@@ -56,9 +56,11 @@ extern "C" {
 #define SHT_ERR_TOO_LARGE        8  /* request exceeds a fixed capacity          */
 
 /* precision modes of the Legendre contraction */
-#define SHT_PREC_FP64  0  /* plain FP64 on CUDA cores                             */
-#define SHT_PREC_SPLIT 1  /* FP64 operands sliced into low-precision integer
-                             pieces, exact tensor-core products, FP64 recombine  */
+#define SHT_PREC_FP64  0  /* FP64 operands and FP64 products (the FP64 tensor
+                             path, mma.sync f64), FP64 accumulation            */
+#define SHT_PREC_SPLIT 1  /* FP64 operands as six signed 8-bit digits, exact
+                             integer digit products on the tcgen05 tensor
+                             cores, FP64 recombination                         */
 
 typedef struct sht_plan_s sht_plan;
 
@@ -396,11 +398,6 @@ SHT_API int sht_last_timing(const sht_plan *plan, float *ms_fft, float *ms_legen
 
 /* Number of kernel launches issued by this library since process start. */
 SHT_API long long sht_launch_count(void);
-
-/* FP64 throughput of the current device in TFLOP/s, measured by two
- * dependency-free loops (DFMA, and mma.sync.m8n8k4.f64); the roofline
- * denominator of the FP64 Legendre contraction.  Either pointer may be NULL. */
-SHT_API int sht_probe_fp64_tflops(double *tflops_dfma, double *tflops_dmma);
 
 #ifdef __cplusplus
 }

@@ -1,8 +1,9 @@
-"""Split-precision Legendre contraction (BF16 digit products on tcgen05, FP64
-recombination) through the C-ABI, against the CPU oracle and the FP64 path.
+"""Split-precision Legendre contraction (signed 8-bit digit products on
+tcgen05, exact integer level sums, FP64 recombination) through the C-ABI,
+against the CPU oracle and the FP64 path.
 
 Tolerance: 1e-11 per-field normwise relative error, the same bar as the plain
-FP64 path (the error-free splitting keeps about 46 bits per operand).
+FP64 path (the digits keep 46 bits per operand below its row or column bound).
 """
 import numpy as np
 import pytest
@@ -107,18 +108,23 @@ def test_split_t341_matches_fp64(plan_cache):
     assert relerr(back, w) < TOL
 
 
-def test_split_rejects_grids_it_does_not_cover(plan_cache):
-    """More than 256 half-latitudes would put more than 256 terms into an
-    exact FP32 level sum."""
-    P = pkg()
-    gpu, _ = plan_cache(64, 1024, 21)
+def test_split_many_latitudes_vs_oracle(plan_cache):
+    """512 half-latitudes: the analysis contraction runs over eight K chunks,
+    with the column exponents from a first pass over all of them."""
+    P, W = pkg(), workloads()
+    gpu, ora = plan_cache(64, 1024, 21)
+    rng = np.random.default_rng(12)
+    w = W.seeded_spectra(21, 6, 1.5, rng=rng)
+    x = rng.standard_normal((6, 1024, 64))
     gpu.set_precision(P.SHT_PREC_SPLIT)
     try:
-        with pytest.raises(P.SpmlError) as ei:
-            gpu.xya_wa(np.zeros((1, gpu.lm)))
-        assert ei.value.status == 2
+        g = gpu.xya_wa(w)
+        back = gpu.wa_xya(x)
+        gpu.synchronize()
     finally:
         gpu.set_precision(P.SHT_PREC_FP64)
+    assert relerr(g, ora.xya_wa(w)) < TOL
+    assert relerr(back, ora.wa_xya(x)) < TOL
 
 
 def _trel(a, b) -> float:
