@@ -69,6 +69,13 @@ __host__ __device__ inline int exp_of(double mx)
   return e < kExpMin ? kExpMin : e;
 }
 
+// the same from the high word of the largest magnitude (sign bit clear)
+__host__ __device__ inline int exp_of_hi(int hi)
+{
+  const int e = (hi >> 20) - 1022;
+  return e < kExpMin ? kExpMin : e;
+}
+
 // 2^e for -1022 <= e <= 1023
 __host__ __device__ inline double pow2(int e) { return bits2d((int64_t)(e + 1023) << 52); }
 

@@ -272,11 +272,14 @@ __device__ bool wait_ph(const Ctl &c, int b, uint32_t parity)
     }
   }
 }
-// the same for a whole warp, with one outcome for all its lanes
+// the same for a whole warp: lane 0 waits (acquiring the phase), and the
+// shuffle both gives every lane the outcome and orders the lanes' later
+// accesses after lane 0's acquire
 __device__ __forceinline__ bool warp_wait(const Ctl &c, int b, uint32_t parity)
 {
-  const bool ok = wait_ph(c, b, parity);
-  return __all_sync(0xffffffffu, ok) != 0;
+  int ok = 0;
+  if ((threadIdx.x & 31) == 0) ok = wait_ph(c, b, parity) ? 1 : 0;
+  return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
 // No memory clobber: nothing in the kernel reads these outputs, and the
@@ -366,12 +369,17 @@ __device__ void role_mma(const I8Args &a, const Ctl &c, uint32_t As, uint32_t Ps
         tc::fence_after();
       }
       const uint32_t d0 = tbase + (uint32_t)(set * kSetCols);
+      // descriptors built once; the start address (bits 0..13, in 16-byte
+      // units, below 256 KB of shared memory) then steps by plain adds
+      const uint64_t ad0 = tc::smem_desc(As + st * kStageA, 128, 512);
+      const uint64_t bd0 = tc::smem_desc(pb, 128, 512);
+      const uint32_t id0 = tc::idesc_s8_s32(kM, 0);
       // MMA of data digit sd against table digits [t0, t0 + nt): level sums
       // L = sd + t go to accumulator columns from (sd + t0) npad on
       auto mma = [&](int ks, int sd, int t0, int nt, uint32_t acc) {
-        const uint64_t ad = tc::smem_desc(As + st * kStageA + sd * kTileA + ks * 256, 128, 512);
-        const uint64_t bd = tc::smem_desc(pb + t0 * npad * kKC + ks * 256, 128, 512);
-        tc::mma_s8(d0 + (uint32_t)((sd + t0) * npad), ad, bd, tc::idesc_s8_s32(kM, nt * npad), acc);
+        const uint64_t ad = ad0 + (uint64_t)((sd * kTileA + ks * 256) >> 4);
+        const uint64_t bd = bd0 + (uint64_t)((t0 * npad * kKC + ks * 256) >> 4);
+        tc::mma_s8(d0 + (uint32_t)((sd + t0) * npad), ad, bd, id0 | ((uint32_t)(nt * npad) >> 3) << 17, acc);
       };
       static_assert(kLevels == kDigitsTable + 1, "data digits 0 and 1 pair with every table digit");
       for (int ks = 0; ks < nks; ++ks) {
@@ -450,7 +458,9 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
       const int cl = 8 * (warp - R::kConv0) + c8 + 8 * R::kConvW * ps;  // complex column within the tile
       const int col = u.col0 + cl;
       const bool cv = col < a.ncol;
-      double mr = 0.0, mi = 0.0;
+      // the exponent of a column's largest magnitude is that of the largest
+      // high word (sign cleared): integer maxima, no FP64 chain
+      int mr = 0, mi = 0;
       if (first && u.nch > 1) {
         // column exponents over every K chunk of the sub-item, before this
         // chunk's values take their registers
@@ -462,8 +472,8 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
             for (int i = 0; i < 4; ++i) y[i] = load1<INV>(a, u, col, cv, kk + i0 + i);
 #pragma unroll
             for (int i = 0; i < 4; ++i) {
-              mr = fmax(mr, fabs(y[i].x));
-              mi = fmax(mi, fabs(y[i].y));
+              mr = max(mr, __double2hiint(y[i].x) & 0x7FFFFFFF);
+              mi = max(mi, __double2hiint(y[i].y) & 0x7FFFFFFF);
             }
           }
         }
@@ -472,17 +482,27 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
       load16<INV>(a, u, col, cv, k0, x);
       if (first) {
         if (u.nch == 1) {
+          int hr[8], hi[8];
 #pragma unroll
-          for (int i = 0; i < 16; ++i) {
-            mr = fmax(mr, fabs(x[i].x));
-            mi = fmax(mi, fabs(x[i].y));
+          for (int i = 0; i < 8; ++i) {
+            hr[i] = max(__double2hiint(x[i].x) & 0x7FFFFFFF, __double2hiint(x[i + 8].x) & 0x7FFFFFFF);
+            hi[i] = max(__double2hiint(x[i].y) & 0x7FFFFFFF, __double2hiint(x[i + 8].y) & 0x7FFFFFFF);
           }
+#pragma unroll
+          for (int w = 4; w >= 1; w >>= 1)
+#pragma unroll
+            for (int i = 0; i < w; ++i) {
+              hr[i] = max(hr[i], hr[i + w]);
+              hi[i] = max(hi[i], hi[i + w]);
+            }
+          mr = hr[0];
+          mi = hi[0];
         }
-        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, 8));
-        mr = fmax(mr, __shfl_xor_sync(0xffffffffu, mr, 16));
-        mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, 8));
-        mi = fmax(mi, __shfl_xor_sync(0xffffffffu, mi, 16));
-        const int e_r = i8::exp_of(mr), e_i = i8::exp_of(mi);
+        mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, 8));
+        mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, 16));
+        mi = max(mi, __shfl_xor_sync(0xffffffffu, mi, 8));
+        mi = max(mi, __shfl_xor_sync(0xffffffffu, mi, 16));
+        const int e_r = i8::exp_of_hi(mr), e_i = i8::exp_of_hi(mi);
         if (ps) { er1 = e_r; ei1 = e_i; } else { er0 = e_r; ei0 = e_i; }
         if (q == 0) {
           exps[slot * kM + 2 * cl] = e_r;
