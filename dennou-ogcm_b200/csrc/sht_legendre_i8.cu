@@ -38,9 +38,9 @@
 // and an abort flag that every role polls, and the CTA unwinds (waiting,
 // again bounded, for its own MMAs and copies) and frees its TMEM.
 //
-// Sub-items whose output fits two segments convert their data once for all
-// segments (T85 and below); larger ones convert per (segment, K chunk), and
-// their column exponents come from a first pass over all chunks.
+// A sub-item's data are converted once per group of two output segments
+// (once in all at T85 and below), K chunk by K chunk; when K spans several
+// chunks, the column exponents come from a first pass over all of them.
 #include "sht_internal.h"
 #include "sht_tc.cuh"
 #include "sht_i8digits.cuh"
@@ -184,11 +184,11 @@ __host__ __device__ inline size_t lut_bytes(int N, int npairs)
 }
 
 // One unit of work: a K chunk of a sub-item (band m, parity p, column tile),
-// for all its segments (grouped) or for one of them.
+// for a group of at most two of its segments (the two accumulator sets).
 struct Unit {
   int g;                  // sub-item: item g / 4, band/parity g % 4
-  int m, p, Rp, K, nrow, nseg, nch, grouped;
-  int seg, ch;            // first segment of this unit, K chunk
+  int m, p, Rp, K, nrow, nseg, nch;
+  int seg, ch;            // first segment of this unit's group, K chunk
   int col0;
   int sub_count;          // sub-items this CTA began before this one
   int seg_base;           // segments this CTA began before this sub-item
@@ -210,7 +210,6 @@ __device__ __forceinline__ bool setup_sub(const I8Args &a, const Lut &t, int g, 
   u.nrow = INV ? a.JH : u.Rp;
   u.nseg = nseg_of(u.nrow);
   u.nch = (u.K + kKC - 1) / kKC;
-  u.grouped = u.nseg <= 2;
   u.seg = 0;
   u.ch = 0;
   u.col0 = (item % a.ntiles) * (kM / 2);
@@ -237,7 +236,7 @@ __device__ __forceinline__ bool next_unit(const I8Args &a, const Lut &t, int g1,
 {
   if (++u.ch < u.nch) return true;
   u.ch = 0;
-  if (!u.grouped && ++u.seg < u.nseg) return true;
+  if ((u.seg += 2) < u.nseg) return true;
   const int sc = u.sub_count + 1, sb = u.seg_base + u.nseg;
   for (int g = u.g + 1; g < g1; ++g)
     if (setup_sub<INV>(a, t, g, u)) {
@@ -328,7 +327,7 @@ __device__ void role_producer(const I8Args &a, const Ctl &c, unsigned char *Ps, 
   for (; have; have = next_unit<INV>(a, t, g1, u), ++k) {
     const int st = k & 1;
     if (k >= 2 && !wait_ph(c, B_PEMPTY + st, ((k >> 1) - 1) & 1)) break;
-    const int s0 = u.grouped ? 0 : u.seg, s1 = u.grouped ? u.nseg : u.seg + 1;
+    const int s0 = u.seg, s1 = min(u.seg + 2, u.nseg);
     const int npt = npad_total(u.nrow);
     const uint8_t *src = a.tab + u.toff + (long long)u.ch * kDigitsTable * kKC * npt +
                          (long long)s0 * kDigitsTable * kKC * kSeg;
@@ -355,7 +354,7 @@ __device__ void role_mma(const I8Args &a, const Ctl &c, uint32_t As, uint32_t Ps
     if (!wait_ph(c, B_PFULL + st, (k >> 1) & 1)) break;
     if (!wait_ph(c, B_DFULL + st, (k >> 1) & 1)) break;
     tc::fence_after();
-    const int s0 = u.grouped ? 0 : u.seg, s1 = u.grouped ? u.nseg : u.seg + 1;
+    const int s0 = u.seg, s1 = min(u.seg + 2, u.nseg);
     const int kvalid = min(kKC, u.K - u.ch * kKC);
     const int nks = (kvalid + 31) / 32;
     uint32_t pb = Ps + st * kStageP;
@@ -509,7 +508,7 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
           exps[slot * kM + 2 * cl + 1] = e_i;
         }
       }
-      if (!INV && u.grouped && u.nch == 1 && cv && (a.JH & 7) == 0) {
+      if (!INV && u.nseg <= 2 && u.nch == 1 && cv && (a.JH & 7) == 0) {
         // each 128-byte line of this column's run is read once, by this thread:
         // drop it from L2 without a write-back (the values are in registers)
         const double2 *src = a.F + ((long long)u.m * a.ncol + col) * a.J + u.p * a.JH + k0;
@@ -581,7 +580,7 @@ __device__ void role_epilogue(const I8Args &a, const Ctl &c, const int *exps, ui
       if (lane == 0) tc::mbar_arrive(c.bar + B_EEMPTY + slot);
     }
     if (u.ch != u.nch - 1) continue;  // no segment completes in this unit
-    const int s0 = u.grouped ? 0 : u.seg, s1 = u.grouped ? u.nseg : u.seg + 1;
+    const int s0 = u.seg, s1 = min(u.seg + 2, u.nseg);
     const double *frow = a.tfac + u.teoff;
     const double fcol = i8::pow2(ecol < 1023 ? ecol : 1023);
     const bool fast = u.K <= 64;
