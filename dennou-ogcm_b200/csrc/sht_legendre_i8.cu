@@ -261,8 +261,9 @@ __device__ bool wait_ph(const Ctl &c, int b, uint32_t parity)
   if (tc::mbar_try(addr, parity)) return true;
   const uint64_t t0 = tc::globaltimer_ns();
   while (true) {
-    // sleeps inside the call (up to 20 us) until the phase completes
-    if (tc::mbar_try_sleep(addr, parity, 20000u)) return true;
+    // the thread is suspended inside the call until the phase completes (or
+    // 1 ms passes), so a waiting warp takes no issue slots from working ones
+    if (tc::mbar_try_sleep(addr, parity, 1000000u)) return true;
     if (*c.abort_flag) return false;
     if (tc::globaltimer_ns() - t0 > kWaitLimit) {
       *c.abort_flag = 1;
