@@ -123,6 +123,9 @@ struct sht_plan_s {
 
   // split-precision tables (built lazily)
   void *tc_tables = nullptr;
+  // device address of the allocation-free entry point's fixed scratch array
+  // on this plan's device (looked up on that entry point's first call)
+  void *noalloc_scratch = nullptr;
 
   // graphs of staged host-pointer calls (SHT_OPT_HOST_GRAPHS), the stream
   // they are captured on, and the generation of the buffers they name

@@ -31,7 +31,6 @@
 #include "sht_internal.h"
 
 #include <cstdio>
-#include <mutex>
 
 #define SHT_NOALLOC_SCRATCH_BYTES (32ull << 20)
 
@@ -39,25 +38,18 @@ namespace {
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[SHT_NOALLOC_SCRATCH_BYTES];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-void *g_scratch_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on `dev` (which must be current).
-int scratch_address(int dev, void **out)
+// Device address of the scratch array on the plan's device (which must be
+// current).  The address is kept in the plan, so a plan created after a
+// device reset looks it up again.
+int scratch_address(sht_plan *p, void **out)
 {
-  if (dev < 0 || dev >= kMaxDevices) {
-    sht::set_error("noalloc: device ordinal out of range");
-    return SHT_ERR_INVALID_ARG;
-  }
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  if (!p->noalloc_scratch) {
     void *ptr = nullptr;
     cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
     if (e != cudaSuccess) return sht::cuda_fail(e, "noalloc: cudaGetSymbolAddress(scratch)");
-    g_scratch_addr[dev] = ptr;
+    p->noalloc_scratch = ptr;
   }
-  *out = g_scratch_addr[dev];
+  *out = p->noalloc_scratch;
   return SHT_OK;
 }
 
@@ -78,8 +70,7 @@ extern "C" SHT_API int sht_wa_xya_dev_noalloc(sht_plan *p, const double *xya, in
     set_error("noalloc: bad argument");
     return SHT_ERR_INVALID_ARG;
   }
-  if (nb == 0) return SHT_OK;
-  if ((reinterpret_cast<uintptr_t>(xya) & 15u) != 0) {
+  if (nb > 0 && (reinterpret_cast<uintptr_t>(xya) & 15u) != 0) {
     set_error("noalloc: device grid arrays must be 16-byte aligned");
     return SHT_ERR_INVALID_ARG;
   }
@@ -110,8 +101,8 @@ extern "C" SHT_API int sht_wa_xya_dev_noalloc(sht_plan *p, const double *xya, in
     return SHT_ERR_CUDA;
   }
   void *base = nullptr;
-  int rc = scratch_address(p->device, &base);
-  if (!rc) {
+  int rc = scratch_address(p, &base);
+  if (!rc && nb > 0) {
     double2 *F = static_cast<double2 *>(base);
     double2 *S = reinterpret_cast<double2 *>(static_cast<char *>(base) + fbytes);
     cudaStream_t s = p->stream;

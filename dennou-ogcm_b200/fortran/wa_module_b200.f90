@@ -33,12 +33,18 @@ module wa_module_b200
   public :: b200_wa_Diffuse
   public :: b200_wa_AlphaOptrProd_xya, b200_xya_HGrad_wa, b200_xya_HGrad_xya, b200_xya_FluxDiv_xya
   public :: b200_wa_xyz_section, b200_xyz_wa_section
+  ! legacy spellings of the horizontal transforms of the sogcm SpmlUtil_mod
+  ! (model/old/sogcm/util/SpmlUtil_mod.f90:75-84,308-344,529-679)
+  public :: xyz_wz, wz_xyz, wt_xyt
+  public :: wz_AlphaOptr_xyz, xyz_AlphaOptr_wz
+  public :: w_Lapla2D_w, wz_Lapla2D_wz, w_InvLapla2D_w, wz_InvLapla2D_wz
 
   integer, parameter :: SHT_OK = 0
   character(*), parameter :: module_name = 'wa_module_b200'
 
   type(c_ptr), save :: plan = c_null_ptr
   integer, save :: im = 0, jm = 0, nm = 0, lm = 0
+  real(DP), save :: radius_ = 1.0_DP   ! planetary radius given to wa_Initial
 
   real(DP), save, allocatable :: x_Lon(:), y_Lat(:), x_Lon_Weight(:), y_Lat_Weight(:)
   real(DP), save, allocatable :: xy_Lon(:,:), xy_Lat(:,:)
@@ -241,6 +247,7 @@ contains
     integer(c_int) :: ci, cj, cn, cl
     a = 1.0_DP
     if (present(radius)) a = radius
+    radius_ = a
     call check(sht_init(int(i_in, c_int), int(j_in, c_int), int(k_in, c_int), int(n_in, c_int), &
          real(a, c_double), plan), 'wa_Initial')
     ! the plan fixes nm (nm = -1 selects the default) and lm: (nm+1)**2, or
@@ -509,5 +516,79 @@ contains
     call check(sht_synthesis(plan, wa, int(size(wa, 1), c_int), int(size(wa, 2), c_int), c_loc(xyz(is, js, 1)), &
          int(size(xyz, 1), c_int), int(size(xyz, 2), c_int), md), 'xyz_wa_section')
   end subroutine b200_xyz_wa_section
+
+  ! ------------------------------------------------------------------------
+  ! Legacy spellings (sogcm SpmlUtil_mod): the same batched transforms with the
+  ! vertical index 0:km last (wz, xyz) or 0:tm (wt, xyt on Chebyshev points).
+
+  !> xyz_wz = xya_wa (model/old/sogcm/util/SpmlUtil_mod.f90:308-320)
+  function xyz_wz(wz)
+    real(DP), intent(in) :: wz(:,0:)
+    real(DP) :: xyz_wz(0:im-1, jm, 0:size(wz, 2) - 1)
+    call check(sht_xya_wa(plan, wz, int(size(wz, 2), c_int), xyz_wz), 'xyz_wz')
+  end function xyz_wz
+
+  !> wz_xyz = wa_xya (model/old/sogcm/util/SpmlUtil_mod.f90:322-333)
+  function wz_xyz(xyz)
+    real(DP), intent(in) :: xyz(:,:,0:)
+    real(DP) :: wz_xyz(lm, 0:size(xyz, 3) - 1)
+    call check(sht_wa_xya(plan, xyz, int(size(xyz, 3), c_int), wz_xyz), 'wz_xyz')
+  end function wz_xyz
+
+  !> wt_xyt = wa_xya on the Chebyshev levels (model/old/sogcm/util/SpmlUtil_mod.f90:335-346)
+  function wt_xyt(xyt)
+    real(DP), intent(in) :: xyt(:,:,0:)
+    real(DP) :: wt_xyt(lm, 0:size(xyt, 3) - 1)
+    call check(sht_wa_xya(plan, xyt, int(size(xyt, 3), c_int), wt_xyt), 'wt_xyt')
+  end function wt_xyt
+
+  !> (wa_DivLambda_xya(A) + wa_DivMu_xya(B)) / Radius (model/old/sogcm/util/SpmlUtil_mod.f90:529-543)
+  function wz_AlphaOptr_xyz(xyz_A, xyz_B)
+    real(DP), intent(in) :: xyz_A(:,:,0:), xyz_B(:,:,0:)
+    real(DP) :: wz_AlphaOptr_xyz(lm, 0:size(xyz_A, 3) - 1)
+    call check(sht_wa_alphaoptr_xya(plan, xyz_A, xyz_B, int(size(xyz_A, 3), c_int), wz_AlphaOptr_xyz), &
+         'wz_AlphaOptr_xyz')
+  end function wz_AlphaOptr_xyz
+
+  !> (xya_GradLambda_wa(A) + xya_GradMu_wa(B)) / (Radius cos^2 phi)
+  !> (model/old/sogcm/util/SpmlUtil_mod.f90:561-577)
+  function xyz_AlphaOptr_wz(wz_A, wz_B)
+    real(DP), intent(in) :: wz_A(:,0:), wz_B(:,0:)
+    real(DP) :: xyz_AlphaOptr_wz(0:im-1, jm, 0:size(wz_A, 2) - 1)
+    call check(sht_xya_alphaoptr_wa(plan, wz_A, wz_B, int(size(wz_A, 2), c_int), xyz_AlphaOptr_wz), &
+         'xyz_AlphaOptr_wz')
+  end function xyz_AlphaOptr_wz
+
+  !> w_Lapla_w / Radius**2 (model/old/sogcm/util/SpmlUtil_mod.f90:596-615)
+  function w_Lapla2D_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: w_Lapla2D_w(lm)
+    call check(sht_wa_lapla_wa(plan, w, 1_c_int, w_Lapla2D_w), 'w_Lapla2D_w')
+    w_Lapla2D_w = w_Lapla2D_w / radius_**2
+  end function w_Lapla2D_w
+
+  !> wa_Lapla_wa / Radius**2 (model/old/sogcm/util/SpmlUtil_mod.f90:617-636)
+  function wz_Lapla2D_wz(wz)
+    real(DP), intent(in) :: wz(:,0:)
+    real(DP) :: wz_Lapla2D_wz(lm, 0:size(wz, 2) - 1)
+    call check(sht_wa_lapla_wa(plan, wz, int(size(wz, 2), c_int), wz_Lapla2D_wz), 'wz_Lapla2D_wz')
+    wz_Lapla2D_wz = wz_Lapla2D_wz / radius_**2
+  end function wz_Lapla2D_wz
+
+  !> w_LaplaInv_w * Radius**2 (model/old/sogcm/util/SpmlUtil_mod.f90:660-679)
+  function w_InvLapla2D_w(w)
+    real(DP), intent(in) :: w(lm)
+    real(DP) :: w_InvLapla2D_w(lm)
+    call check(sht_wa_laplainv_wa(plan, w, 1_c_int, w_InvLapla2D_w), 'w_InvLapla2D_w')
+    w_InvLapla2D_w = w_InvLapla2D_w * radius_**2
+  end function w_InvLapla2D_w
+
+  !> wa_LaplaInv_wa * Radius**2 (model/old/sogcm/util/SpmlUtil_mod.f90:638-657)
+  function wz_InvLapla2D_wz(wz)
+    real(DP), intent(in) :: wz(:,0:)
+    real(DP) :: wz_InvLapla2D_wz(lm, 0:size(wz, 2) - 1)
+    call check(sht_wa_laplainv_wa(plan, wz, int(size(wz, 2), c_int), wz_InvLapla2D_wz), 'wz_InvLapla2D_wz')
+    wz_InvLapla2D_wz = wz_InvLapla2D_wz * radius_**2
+  end function wz_InvLapla2D_wz
 
 end module wa_module_b200

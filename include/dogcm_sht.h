@@ -323,8 +323,12 @@ SHT_API int sht_synthesis_dev(sht_plan *plan, const double *wa, int ldw, int nb,
  * (32 MiB), held by every GPU that loads the library until exit.  It calls no
  * allocator.  A batch needing more scratch returns SHT_ERR_TOO_LARGE.  All
  * calls share that array, so calls that overlap on the GPU race: order them
- * on one stream.  The first call on each device looks up the array's address
- * (cudaGetSymbolAddress), so make it before any stream capture.  The plan
+ * on one stream.  The first call on a plan looks up the array's address
+ * (cudaGetSymbolAddress); on a device's first lookup the driver loads the
+ * array's module and reserves the array (CUDA's default lazy loading).  A
+ * call with nb = 0 does only that set-up: make it at start-up, before another
+ * pool takes the GPU's memory and before any stream capture.  Stage timing
+ * (sht_last_timing) does not cover this entry point.  The plan
  * must already exist (sht_init allocates its tables); in split precision,
  * so must its digit tables, which the plan's first split-precision call of an
  * ordinary entry point allocates (until then this returns

@@ -50,13 +50,47 @@ def test_noalloc_matches_device_entry_point_twice():
             ref = torch.empty((nb, (N + 1) ** 2), dtype=torch.float64, device="cuda")
             out = torch.full_like(ref, float("nan"))
             assert lib.sht_wa_xya_dev(sht._h, VP(grid.data_ptr()), nb, VP(ref.data_ptr())) == 0
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             st = lib.sht_wa_xya_dev_noalloc(sht._h, VP(grid.data_ptr()), nb, VP(out.data_ptr()))
             assert st == 0, lib.sht_last_error()
             torch.cuda.synchronize()
+            if call == 1:
+                # the call's whole contract: no device memory is taken (the
+                # first call may still load the module that holds the array)
+                assert torch.cuda.mem_get_info()[0] == free_before, "the call allocated device memory"
             o, r = out.cpu().numpy(), ref.cpu().numpy()
             assert np.isfinite(o).all(), f"call {call}: non-finite output"
             assert relerr(o, r) < TOL, f"call {call}: {relerr(o, r)}"
             assert relerr(o, w.cpu().numpy()) < TOL, f"call {call}: round trip"
+    finally:
+        sht.final()
+
+
+def test_noalloc_setup_call_with_no_field_levels():
+    """A call with nb = 0 only looks up the scratch array (loading its module
+    on the device's first lookup), so a host can make it at start-up, before
+    another pool takes the GPU's memory; after it, a real call takes no memory."""
+    import torch
+
+    P, W = pkg(), workloads()
+    lib = _lib()
+    I, J, N = W.GRIDS["T42"]
+    nb = 16
+    sht = P.SpmlUtil(I, J, nb, N, None, 1.0)
+    try:
+        stream = torch.cuda.current_stream()
+        assert lib.sht_set_stream(sht._h, VP(stream.cuda_stream)) == 0
+        assert lib.sht_wa_xya_dev_noalloc(sht._h, None, 0, None) == 0
+        w = torch.from_numpy(W.seeded_spectra(N, nb, 1.5, seed=11)).cuda()
+        grid = sht.xya_wa(w)
+        out = torch.full((nb, (N + 1) ** 2), float("nan"), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        assert lib.sht_wa_xya_dev_noalloc(sht._h, VP(grid.data_ptr()), nb, VP(out.data_ptr())) == 0
+        torch.cuda.synchronize()
+        assert torch.cuda.mem_get_info()[0] == free_before
+        assert relerr(out.cpu().numpy(), w.cpu().numpy()) < TOL
     finally:
         sht.final()
 
