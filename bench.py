@@ -357,6 +357,9 @@ def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
       equation, Q = H cos(phi) T);
     - Redi/GM gradients: xy_HGrad_xy(T) against w_xy then xy_GradLon_w and
       xy_GradLat_w;
+    - momentum products: calc_UVCosLat2VorDiv of cos(phi)(U Vor + Za) and
+      cos(phi)(V Vor + Zb) formed in the load, against the two grids built by
+      torch and then analysed;
     - batched callers: the transform parts of the tracer and momentum
       tendency loops over 60 levels in one call per operator, against the
       same operators called level by level."""
@@ -391,15 +394,24 @@ def bench_fused(P, torch, dev, sht, args, flush, max_over_ranks):
         w = sht.w_xy(T)
         return sht.xy_GradLon_w(w), sht.xy_GradLat_w(w)
 
+    Z = torch.randn(shape, generator=g, dtype=torch.float64, device=dev)
+    cs = torch.cos(torch.as_tensor(sht.y_Lat, dtype=torch.float64, device=dev))[None, :, None]
+
+    def mom_unfused():
+        return sht.calc_UVCosLat2VorDiv(cs * (A * Q + T), cs * (B * Q + Z))
+
     fused_p, ref_p = sht.w_AlphaOptrProd_xy(A, B, Q), prod_unfused()
     (lon, lat), (rlon, rlat) = sht.xy_HGrad_xy(T), hgrad_unfused()
+    (mv, md), (rmv, rmd) = sht.calc_UVCosLat2VorDiv_fma(A, B, Q, T, Z), mom_unfused()
     torch.cuda.synchronize()
     out = {"workload": f"{nb} field-levels on the headline grid, fp64"}
     for name, fused, unfused, err in (
             ("alphaoptr_prod", lambda: sht.w_AlphaOptrProd_xy(A, B, Q), prod_unfused,
              _rel(fused_p.cpu().numpy(), ref_p.cpu().numpy())),
             ("hgrad_xya", lambda: sht.xy_HGrad_xy(T), hgrad_unfused,
-             max(_rel(lon.cpu().numpy(), rlon.cpu().numpy()), _rel(lat.cpu().numpy(), rlat.cpu().numpy())))):
+             max(_rel(lon.cpu().numpy(), rlon.cpu().numpy()), _rel(lat.cpu().numpy(), rlat.cpu().numpy()))),
+            ("momentum_products", lambda: sht.calc_UVCosLat2VorDiv_fma(A, B, Q, T, Z), mom_unfused,
+             max(_rel(mv.cpu().numpy(), rmv.cpu().numpy()), _rel(md.cpu().numpy(), rmd.cpu().numpy())))):
         tf, tu = timeit(fused), timeit(unfused)
         out[name] = {"fused_ms": tf, "unfused_ms": tu, "speedup": tu / tf, "relerr_vs_unfused": err}
     # the same analysis without the products: what the product epilogue adds

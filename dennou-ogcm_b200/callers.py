@@ -48,6 +48,19 @@ def momrhs_vordiv(sp, a, b, c):
     return sp.calc_VorDiv2UV(-div, vor - sp.w_Lapla_w(sp.w_xy(c)))
 
 
+def momrhs_vordiv_fma(sp, u, v, vor, za, zb, c):
+    """The same tendencies from the model's fields instead of xy_A, xy_B:
+
+        xy_A = cos(phi) (Vor U + za),  xy_B = cos(phi) (Vor V + zb)
+
+    (HBEBaroc_hspm_vfvm_mod.f90:394-418; za, zb every other term of the
+    products, e.g. CoriU + VAdvV/H - VRHS_phys + DensEdd GradLat(GeoPot)/(rho a)),
+    with the products formed while the grids load into the longitude
+    transform, so that A and B are never written."""
+    wv, wd = sp.calc_UVCosLat2VorDiv_fma(u, v, vor, za, zb)
+    return sp.calc_VorDiv2UV(-wd, wv - sp.w_Lapla_w(sp.w_xy(c)))
+
+
 def diagnose_vordiv(sp, u, v):
     """Vorticity and divergence grids of HBEDiagnose_VorDiv
     (HBEDiagnose_hspm_vfvm_mod.f90:276-284):

@@ -191,7 +191,8 @@ void finish_timing(sht_plan *p, bool analysis)
 // (with `mul`, every input field-level k is first multiplied point by point by
 // the grid mul + k I J)
 int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const double *g1, int nb,
-                 double *w0, double *w1, const double *mul = nullptr)
+                 double *w0, double *w1, const double *mul = nullptr, const double *add0 = nullptr,
+                 const double *add1 = nullptr)
 {
   const int nin = g1 ? 2 : 1, ncol = nin * nb;
   Workspace ws;
@@ -199,7 +200,7 @@ int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const doubl
   if (rc) return rc;
   cudaStream_t s = p->stream;
   mark(p, 0, s);
-  if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s, nullptr, mul, nb))) return rc;
+  if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s, nullptr, mul, nb, add0, add1))) return rc;
   mark(p, 1, s);
   if ((rc = leg_fwd(p, ws.F, ncol, ws.S, s))) return rc;
   mark(p, 2, s);
@@ -794,8 +795,11 @@ int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
   if (nm == -1) nm = zonal ? (2 * jm - 1) / 3 : (im - 1) / 3;
   int lg = 0;
   while ((1 << lg) < im) ++lg;
-  if (!zonal && (im < 16 || im > 2048 || (1 << lg) != im)) {
-    set_error("init: im must be 1 (axisymmetric) or a power of two in [16, 2048]");
+  const bool pow2 = (1 << lg) == im;
+  // powers of two take the four-step FFT; other even counts (factors 3 and 5,
+  // e.g. 96, 192, 320, 640) the direct transform
+  if (!zonal && (im < 16 || im > 2048 || (!pow2 && (im & 1)))) {
+    set_error("init: im must be 1 (axisymmetric) or even in [16, 2048]");
     return SHT_ERR_UNSUPPORTED_SIZE;
   }
   if (jm < 2 || (jm & 1)) { set_error("init: jm must be even and >= 2"); return SHT_ERR_UNSUPPORTED_SIZE; }
@@ -814,6 +818,7 @@ int sht_init(int im, int jm, int km, int nm, double radius, sht_plan **out)
   if (!p) { set_error("init: host allocation failed"); return SHT_ERR_ALLOC; }
   p->I = im; p->J = jm; p->N = nm; p->K = km; p->JH = jm / 2; p->NC = im / 2; p->radius = radius;
   p->zonal = zonal;
+  p->direct_dft = !zonal && !pow2;
   cudaGetDevice(&p->device);
   int rc = SHT_OK;
   if ((e = cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking)) != cudaSuccess) rc = cuda_fail(e, "stream create");
@@ -1047,6 +1052,67 @@ int sht_vordiv2uv(sht_plan *p, const double *vor, const double *div, int nb, dou
 { return api_host(p, OP_VORDIV2UV, vor, div, nb, u, v); }
 int sht_vordiv2uv_dev(sht_plan *p, const double *vor, const double *div, int nb, double *u, double *v)
 { return api_dev(p, OP_VORDIV2UV, vor, div, nb, u, v); }
+
+// calc_UVCosLat2VorDiv(cos(phi) (x1 q + z1), cos(phi) (x2 q + z2)): the
+// momentum products of the vorticity-divergence tendency, formed while the
+// grids load into the longitude transform.  The two products share q; the
+// cos(phi) factor and the 1 / (1 - mu^2) of the analysis meet in one row scale
+// w_j / (I cos(phi_j)).  z1 and z2 are both given or both null (no sums).
+static int uv_fma_impl(sht_plan *p, const double *x1, const double *x2, const double *q, const double *z1,
+                       const double *z2, int nb, double *vor, double *div, bool host)
+{
+  int rc = check_plan(p);
+  if (rc) return rc;
+  if (nb < 0) { set_error("nb must be >= 0"); return SHT_ERR_INVALID_ARG; }
+  if (nb == 0) return SHT_OK;
+  if (!x1 || !x2 || !q || !vor || !div || (!z1) != (!z2)) {
+    set_error("null array argument (z1 and z2 must be both given or both null)");
+    return SHT_ERR_INVALID_ARG;
+  }
+  auto mis = [](const double *x) { return x && (reinterpret_cast<uintptr_t>(x) & 15u) != 0; };
+  if (!host && (mis(x1) || mis(x2) || mis(q) || mis(z1) || mis(z2))) {
+    set_error("device grid arrays must be 16-byte aligned");
+    return SHT_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lk(p->mtx);
+  DeviceGuard g(p->device);
+  if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
+  if (!host) {
+    rc = run_analysis(p, PACK_VORDIV, RS_FWD_INVCOS, x1, x2, nb, vor, div, q, z1, z2);
+    if (!rc) finish_timing(p, true);
+    return rc;
+  }
+  // host arrays: stage every grid, run, copy both spectra back
+  const size_t ng = (size_t)nb * p->I * p->J, nw = (size_t)nb * p->L;
+  auto al = [](size_t n) { return (n + 31) & ~(size_t)31; };  // whole 256-byte blocks
+  const int nin = z1 ? 5 : 3;
+  if ((rc = ensure_io(p, sizeof(double) * (nin * al(ng) + 2 * al(nw))))) return rc;
+  double *d = static_cast<double *>(p->d_io);
+  const double *hin[5] = {x1, x2, q, z1, z2};
+  cudaStream_t s = p->stream;
+  cudaError_t e;
+  for (int k = 0; k < nin; ++k)
+    if ((e = cudaMemcpyAsync(d + k * al(ng), hin[k], sizeof(double) * ng, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_fail(e, "H2D");
+  double *dv = d + nin * al(ng), *dd = dv + al(nw);
+  rc = run_analysis(p, PACK_VORDIV, RS_FWD_INVCOS, d, d + al(ng), nb, dv, dd, d + 2 * al(ng),
+                    z1 ? d + 3 * al(ng) : nullptr, z1 ? d + 4 * al(ng) : nullptr);
+  if (rc) return rc;
+  if ((e = cudaMemcpyAsync(vor, dv, sizeof(double) * nw, cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(div, dd, sizeof(double) * nw, cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+    return cuda_fail(e, "D2H");
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_fail(e, "transform");
+  if ((rc = device_error_status(p))) return rc;
+  finish_timing(p, true);
+  return SHT_OK;
+}
+
+int sht_uvcoslat2vordiv_fma(sht_plan *p, const double *x1, const double *x2, const double *q, const double *z1,
+                            const double *z2, int nb, double *vor, double *div)
+{ return uv_fma_impl(p, x1, x2, q, z1, z2, nb, vor, div, true); }
+int sht_uvcoslat2vordiv_fma_dev(sht_plan *p, const double *x1, const double *x2, const double *q, const double *z1,
+                                const double *z2, int nb, double *vor, double *div)
+{ return uv_fma_impl(p, x1, x2, q, z1, z2, nb, vor, div, false); }
 
 // ---------------------------------------------------------------- strided
 // Analysis and synthesis of arrays with leading dimensions: the model keeps

@@ -130,6 +130,9 @@ struct FftArgs {
   const double *mul;
   int nmul;
   int mul_pair;    // columns c and nsplit + c share a factor: visit them one after the other
+  // multiply-add mode (with mul): column col becomes col * factor + z, z from
+  // add0 + col I J (col < nsplit) or add1 + (col - nsplit) I J
+  const double *add0, *add1;
 };
 
 // Shared-memory plan of one thread block: the twiddle tables (2 NC entries),
@@ -342,6 +345,15 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
       const double2 q = valid ? __ldg(frow + R2 * n1 + u) : make_double2(0.0, 0.0);
       v[n1] = make_double2(v[n1].x * q.x, v[n1].y * q.y);
     }
+    if (a.add0) {
+      const double *zb = col < a.nsplit ? a.add0 + (long long)col * IJ : a.add1 + (long long)(col - a.nsplit) * IJ;
+      const double2 *zrow = reinterpret_cast<const double2 *>(zb) + (long long)(valid ? j : 0) * NC;
+#pragma unroll
+      for (int n1 = 0; n1 < R1; ++n1) {
+        const double2 z = valid ? __ldg(zrow + R2 * n1 + u) : make_double2(0.0, 0.0);
+        v[n1] = make_double2(v[n1].x + z.x, v[n1].y + z.y);
+      }
+    }
     fwd_tile<A, B, NT>(a, v, cur, stw, stwI, col, h0, j, valid);
     __syncthreads();  // the output runs are read; the next tile reuses the buffer
   }
@@ -530,6 +542,11 @@ __global__ void __launch_bounds__(256) k_zonal_fwd(FftArgs a)
       const double *f = a.mul + (long long)(col % a.nmul) * a.J;
       gn *= f[jn];
       gs *= f[js];
+      if (a.add0) {
+        const double *z = col < a.nsplit ? a.add0 + (long long)col * a.J : a.add1 + (long long)(col - a.nsplit) * a.J;
+        gn += z[jn] * __ldg(a.rowscale + jn);
+        gs += z[js] * __ldg(a.rowscale + js);
+      }
     }
     double2 *F = a.F + (long long)(a.colF0 + col) * a.J;
     F[jh] = make_double2(gn + gs, 0.0);
@@ -551,8 +568,152 @@ __global__ void __launch_bounds__(256) k_zonal_inv(FftArgs a)
   }
 }
 
+// Longitude counts that are not powers of two (factors 3 and 5, as in
+// 96, 192, 320 or 640 points, which ISPACK's FFT covers): the transform by
+// direct summation, G^m = s_j sum_i q_i e^{-2 pi i m i / I} for m <= N and its
+// inverse, with e^{-2 pi i t / I} = twI[t] for t < I/2 and -twI[t - I/2]
+// otherwise.  A block handles four mirrored row pairs of one field-level
+// (eight rows staged in shared memory); the outputs take the same Gs/Ga and
+// E/O layouts as the four-step kernels.
+constexpr int kDftPairs = 4;
+constexpr int kDftThreads = 256;
+
+__device__ __forceinline__ double2 dft_twiddle(const double2 *__restrict__ twI, int t, int NC)
+{
+  const double2 w = __ldg(twI + (t < NC ? t : t - NC));
+  return t < NC ? w : make_double2(-w.x, -w.y);
+}
+
+__global__ void __launch_bounds__(kDftThreads) k_dft_fwd(FftArgs a)
+{
+  extern __shared__ __align__(16) double dsm[];
+  const int I = a.I, NC = I / 2, JH = a.JH, N = a.N;
+  double2 *tw = reinterpret_cast<double2 *>(dsm);  // e^{-2 pi i t / I}, t < I
+  double *rows = dsm + 2 * I;                      // 2 kDftPairs rows of I points
+  for (int t = threadIdx.x; t < I; t += blockDim.x) tw[t] = dft_twiddle(a.twI, t, NC);
+  const int ntile = (JH + kDftPairs - 1) / kDftPairs;
+  const long long ntot = (long long)a.ncol * ntile;
+  const long long IJ = (long long)I * a.J;
+  const long long mstride = (long long)a.ncolF * a.J;
+  for (long long tile = blockIdx.x; tile < ntot; tile += gridDim.x) {
+    const int col = (int)(tile / ntile), h0 = (int)(tile - (long long)col * ntile) * kDftPairs;
+    const double *gb = a.gcol ? a.gcol[col]
+                     : (col < a.nsplit) ? a.g0 + (long long)col * IJ : a.g1 + (long long)(col - a.nsplit) * IJ;
+    const double *fb = a.mul ? a.mul + (long long)(col % a.nmul) * IJ : nullptr;
+    const double *zb = (a.mul && a.add0)
+                           ? (col < a.nsplit ? a.add0 + (long long)col * IJ : a.add1 + (long long)(col - a.nsplit) * IJ)
+                           : nullptr;
+    __syncthreads();  // the previous tile's rows are consumed
+    for (int idx = threadIdx.x; idx < 2 * kDftPairs * I; idx += blockDim.x) {
+      const int r = idx / I, i = idx - r * I, jh = h0 + r % kDftPairs;
+      const int j = r < kDftPairs ? JH + jh : JH - 1 - jh;
+      double v = 0.0;
+      if (jh < JH) {
+        v = gb[(long long)j * I + i];
+        if (fb) v *= fb[(long long)j * I + i];
+        if (zb) v += zb[(long long)j * I + i];
+      }
+      rows[idx] = v;
+    }
+    __syncthreads();
+    for (int o = threadIdx.x; o < kDftPairs * (N + 1); o += blockDim.x) {
+      const int pr = o / (N + 1), m = o - pr * (N + 1), jh = h0 + pr;
+      if (jh >= JH) continue;
+      const double *rn = rows + pr * I, *rs = rows + (kDftPairs + pr) * I;
+      double nr = 0.0, ni = 0.0, sr = 0.0, si = 0.0;
+      int t = 0;
+      for (int i = 0; i < I; ++i) {
+        const double2 w = tw[t];
+        nr = fma(rn[i], w.x, nr);
+        ni = fma(rn[i], w.y, ni);
+        sr = fma(rs[i], w.x, sr);
+        si = fma(rs[i], w.y, si);
+        t += m;
+        if (t >= I) t -= I;
+      }
+      const double scn = __ldg(a.rowscale + JH + jh), scs = __ldg(a.rowscale + JH - 1 - jh);
+      nr *= scn; ni *= scn; sr *= scs; si *= scs;
+      if (m == 0) ni = si = 0.0;
+      double2 *Fb = a.F + (long long)m * mstride + (long long)(a.colF0 + col) * a.J;
+      Fb[jh] = make_double2(nr + sr, ni + si);
+      Fb[JH + jh] = make_double2(nr - sr, ni - si);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kDftThreads) k_dft_inv(FftArgs a)
+{
+  extern __shared__ __align__(16) double dsm[];
+  const int I = a.I, NC = I / 2, JH = a.JH, N = a.N;
+  double2 *tw = reinterpret_cast<double2 *>(dsm);     // e^{+2 pi i t / I}, t < I
+  double2 *g = tw + I;                                // 2 kDftPairs rows of N + 1 coefficients
+  for (int t = threadIdx.x; t < I; t += blockDim.x) {
+    const double2 w = dft_twiddle(a.twI, t, NC);
+    tw[t] = make_double2(w.x, -w.y);
+  }
+  const int ntile = (JH + kDftPairs - 1) / kDftPairs;
+  const long long ntot = (long long)a.ncol * ntile;
+  const long long IJ = (long long)I * a.J;
+  const long long mstride = (long long)a.ncolF * a.J;
+  for (long long tile = blockIdx.x; tile < ntot; tile += gridDim.x) {
+    const int col = (int)(tile / ntile), h0 = (int)(tile - (long long)col * ntile) * kDftPairs;
+    __syncthreads();  // the previous tile's coefficients are consumed
+    // row r < kDftPairs: north = E + O; row kDftPairs + r: south = E - O
+    for (int idx = threadIdx.x; idx < kDftPairs * (N + 1); idx += blockDim.x) {
+      const int pr = idx / (N + 1), m = idx - pr * (N + 1), jh = h0 + pr;
+      double2 e = make_double2(0.0, 0.0), od = e;
+      if (jh < JH) {
+        const double2 *Fb = a.Fc + (long long)m * mstride + (long long)(a.colF0 + col) * a.J;
+        e = Fb[jh];
+        od = Fb[JH + jh];
+      }
+      double2 gn = make_double2(e.x + od.x, e.y + od.y), gs = make_double2(e.x - od.x, e.y - od.y);
+      if (m == 0) gn.y = gs.y = 0.0;
+      g[pr * (N + 1) + m] = gn;
+      g[(kDftPairs + pr) * (N + 1) + m] = gs;
+    }
+    __syncthreads();
+    double *ob = a.ocol ? a.ocol[col]
+               : (col < a.nsplit) ? a.o0 + (long long)col * IJ : a.o1 + (long long)(col - a.nsplit) * IJ;
+    for (int o = threadIdx.x; o < 2 * kDftPairs * I; o += blockDim.x) {
+      const int r = o / I, i = o - r * I, jh = h0 + r % kDftPairs;
+      if (jh >= JH) continue;
+      const int j = r < kDftPairs ? JH + jh : JH - 1 - jh;
+      const double2 *gr = g + r * (N + 1);
+      // q_i = G^0 + 2 Re sum_{m >= 1} G^m e^{i m lambda_i}
+      double acc = 0.0;
+      int t = i;
+      for (int m = 1; m <= N; ++m) {
+        const double2 w = tw[t], c = gr[m];
+        acc = fma(c.x, w.x, fma(-c.y, w.y, acc));
+        t += i;
+        if (t >= I) t -= I;
+      }
+      ob[(long long)j * I + i] = (gr[0].x + 2.0 * acc) * __ldg(a.rowscale + j);
+    }
+  }
+}
+
 namespace {
 constexpr int kFftThreads = 128;
+
+int run_dft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
+{
+  const long long ntiles = (long long)a.ncol * ((p->JH + kDftPairs - 1) / kDftPairs);
+  if (ntiles <= 0) return SHT_OK;
+  const size_t smem = inverse ? sizeof(double2) * ((size_t)p->I + 2 * kDftPairs * (size_t)(p->N + 1))
+                              : sizeof(double) * (2 * (size_t)p->I + 2 * kDftPairs * (size_t)p->I);
+  if (smem > 227 * 1024) { set_error("fft: longitude count too large for the direct transform"); return SHT_ERR_UNSUPPORTED_SIZE; }
+  void (*kern)(FftArgs) = inverse ? k_dft_inv : k_dft_fwd;
+  int occ = 0;
+  cudaError_t e = kernel_setup((const void *)kern, smem, kDftThreads, &occ);
+  if (e != cudaSuccess) return cuda_fail(e, "dft smem attribute");
+  const long long g = (long long)(occ < 1 ? 1 : occ) * (p->num_sms > 0 ? p->num_sms : 1);
+  kern<<<(int)(ntiles < g ? ntiles : g), kDftThreads, smem, s>>>(a);
+  count_launch();
+  e = cudaGetLastError();
+  return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_dft_inv" : "k_dft_fwd");
+}
 
 // Persistent grids: as many blocks as fit on the device at once, never more
 // than there are tiles.
@@ -596,6 +757,7 @@ int dispatch(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t 
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_zonal_inv" : "k_zonal_fwd");
   }
+  if (p->direct_dft) return run_dft(inverse, p, args, s);
   switch (p->NC) {
   case 8: return run_fft<2, 1>(inverse, p, args, s);
   case 16: return run_fft<2, 2>(inverse, p, args, s);
@@ -612,11 +774,13 @@ int dispatch(bool inverse, const sht_plan *p, const FftArgs &args, cudaStream_t 
 
 int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
                    double2 *F, int ncolF, int colF0, int rs, cudaStream_t s, const double *const *gcol,
-                   const double *mul, int nmul)
+                   const double *mul, int nmul, const double *add0, const double *add1)
 {
   FftArgs a{};
   a.gcol = gcol;
   a.mul = mul;
+  a.add0 = mul ? add0 : nullptr;
+  a.add1 = mul ? (add1 ? add1 : add0) : nullptr;
   a.nmul = nmul > 0 ? nmul : 1;
   // the two inputs' tiles of one level run back to back, so the level's
   // factor grid comes from L2 the second time

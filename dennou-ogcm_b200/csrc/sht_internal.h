@@ -33,7 +33,8 @@ enum RowScale : int {
   RS_INV_INVCOS = 3,    // synthesis: 1 / cos(phi_j)
   RS_INV_INVA1MMU2 = 4, // synthesis: 1 / (a (1 - mu_j^2))
   RS_INV_INVACOS = 5,   // synthesis: 1 / (a cos(phi_j))
-  RS_COUNT = 6
+  RS_FWD_INVCOS = 6,    // analysis: w_j / (I cos(phi_j)) = w_j cos(phi_j) / (I (1 - mu_j^2))
+  RS_COUNT = 7
 };
 
 // Spectral-side operators applied between the SPML layout and the internal one.
@@ -87,6 +88,7 @@ struct sht_plan_s {
   cudaStream_t copy_in = nullptr, copy_out = nullptr;
   cudaEvent_t chunk_ev[16] = {};
   bool zonal = false;  // im = 1: the axisymmetric (m = 0) transform of wa_zonal_module, lm = nm + 1
+  bool direct_dft = false;  // im not a power of two: longitude transform by direct summation
   int M = 0;           // orders transformed: N + 1, or 1 for a zonal plan
   int precision = SHT_PREC_FP64;
   int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent
@@ -162,7 +164,8 @@ int build_tables(sht_plan *p);
 // scaled per row by rowscale table `rs`.
 int launch_fft_fwd(const sht_plan *p, const double *g0, const double *g1, int nsplit, int ncol,
                    double2 *F, int ncolF, int colF0, int rs, cudaStream_t s,
-                   const double *const *gcol = nullptr, const double *mul = nullptr, int nmul = 0);
+                   const double *const *gcol = nullptr, const double *mul = nullptr, int nmul = 0,
+                   const double *add0 = nullptr, const double *add1 = nullptr);
 // F -> grid (two destinations split at nsplit, or column c at ocol[c]),
 // scaled per row by `rs`.
 int launch_fft_inv(const sht_plan *p, const double2 *F, int ncolF, int colF0, int ncol,

@@ -172,6 +172,7 @@ int build_tables(sht_plan *p)
     rs[RS_INV_INVCOS * J + j] = 1.0 / c;
     rs[RS_INV_INVA1MMU2 * J + j] = 1.0 / (p->radius * c2);
     rs[RS_INV_INVACOS * J + j] = 1.0 / (p->radius * c);
+    rs[RS_FWD_INVCOS * J + j] = w / (I * c);
   }
   if ((rc = dalloc(&p->d_rowscale, rs.size()))) return rc;
   if ((e = cudaMemcpyAsync(p->d_rowscale, rs.data(), sizeof(double) * rs.size(), cudaMemcpyHostToDevice, p->stream)) != cudaSuccess)

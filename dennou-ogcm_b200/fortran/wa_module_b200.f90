@@ -29,7 +29,7 @@ module wa_module_b200
   public :: w_Lapla_w, w_LaplaInv_w
   public :: AvrLonLat_xy, IntLonLat_xy, ya_AvrLon_xya, ya_IntLon_xya
   public :: b200_wa_AlphaOptr_xya, b200_xya_AlphaOptr_wa
-  public :: b200_calc_UVCosLat2VorDiv, b200_calc_VorDiv2UV
+  public :: b200_calc_UVCosLat2VorDiv, b200_calc_VorDiv2UV, b200_calc_MomProd2VorDiv
   public :: b200_wa_Diffuse
   public :: b200_wa_AlphaOptrProd_xya, b200_xya_HGrad_wa, b200_xya_HGrad_xya, b200_xya_FluxDiv_xya
   public :: b200_wa_xyz_section, b200_xyz_wa_section
@@ -178,6 +178,12 @@ module wa_module_b200
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: plan; real(c_double), intent(in) :: a(*), b(*), q(*)
       integer(c_int), value :: nb; real(c_double), intent(out) :: w(*)
+    end function
+    integer(c_int) function sht_uvcoslat2vordiv_fma(plan, x1, x2, q, z1, z2, nb, vor, div) &
+         bind(C, name='sht_uvcoslat2vordiv_fma')
+      import :: c_int, c_double, c_ptr
+      type(c_ptr), value :: plan; real(c_double), intent(in) :: x1(*), x2(*), q(*), z1(*), z2(*)
+      integer(c_int), value :: nb; real(c_double), intent(out) :: vor(*), div(*)
     end function
     integer(c_int) function sht_xya_hgrad_wa(plan, w, nb, glon, glat) bind(C, name='sht_xya_hgrad_wa')
       import :: c_int, c_double, c_ptr
@@ -456,6 +462,16 @@ contains
     call check(sht_wa_alphaoptr_prod_xya(plan, xya_A, xya_B, xya_Q, int(size(xya_A, 3), c_int), &
          b200_wa_AlphaOptrProd_xya), 'wa_AlphaOptrProd_xya')
   end function b200_wa_AlphaOptrProd_xya
+
+  !> calc_UVCosLat2VorDiv(cos(phi) (X1 Q + Z1), cos(phi) (X2 Q + Z2)): xy_A, xy_B of
+  !> HBEBaroc_MOMRHS_VorDivForm (dynamics/hspm_vfvm/HBEBaroc_hspm_vfvm_mod.f90:394-418)
+  !> formed in the longitude transform (Q = Vor, X1 = U, X2 = V, Z1, Z2 the other terms)
+  subroutine b200_calc_MomProd2VorDiv(xya_X1, xya_X2, xya_Q, xya_Z1, xya_Z2, wa_Vor, wa_Div)
+    real(DP), intent(in) :: xya_X1(:,:,:), xya_X2(:,:,:), xya_Q(:,:,:), xya_Z1(:,:,:), xya_Z2(:,:,:)
+    real(DP), intent(out) :: wa_Vor(:,:), wa_Div(:,:)
+    call check(sht_uvcoslat2vordiv_fma(plan, xya_X1, xya_X2, xya_Q, xya_Z1, xya_Z2, &
+         int(size(xya_X1, 3), c_int), wa_Vor, wa_Div), 'calc_MomProd2VorDiv')
+  end subroutine b200_calc_MomProd2VorDiv
 
   !> xya_GradLon_wa and xya_GradLat_wa of one spectrum, one synthesis
   subroutine b200_xya_HGrad_wa(wa, xya_GradLon, xya_GradLat)

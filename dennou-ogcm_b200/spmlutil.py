@@ -102,6 +102,7 @@ def load_library(path: str | None = None):
             getattr(lib, name + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, _VP]
     for suf in ("", "_dev"):
         getattr(lib, "sht_wa_alphaoptr_prod_xya" + suf).argtypes = [_VP, _VP, _VP, _VP, ctypes.c_int, _VP]
+        getattr(lib, "sht_uvcoslat2vordiv_fma" + suf).argtypes = [_VP] * 6 + [ctypes.c_int, _VP, _VP]
     for suf in ("", "_dev"):
         getattr(lib, "sht_wa_diffuse" + suf).argtypes = [_VP, _VP, ctypes.c_int, _VP, ctypes.c_double, _VP]
     for suf in ("", "_dev"):
@@ -275,8 +276,8 @@ class SpmlUtil:
         x0 = ins[0]
         nb, batched = (self._grid_shape(x0) if x0.shape[-1] == self.im and x0.ndim >= 2 and x0.shape[-2] == self.jm
                        else self._spec_shape(x0))
-        for x in ins[1:]:
-            if tuple(x.shape) != tuple(x0.shape):
+        for x in ins[1:]:  # None: an optional input left out (a null pointer)
+            if x is not None and tuple(x.shape) != tuple(x0.shape):
                 raise SpmlError(1, name, "input shapes differ")
         if out_kind == "grid":
             oshape = (nb, self.jm, self.im)
@@ -288,17 +289,17 @@ class SpmlUtil:
             oshape = (nb, self.jm)
         if _is_torch_cuda(x0):
             import torch
-            ins = [x.contiguous() for x in ins]
-            if any(x.dtype != torch.float64 for x in ins):
+            ins = [None if x is None else x.contiguous() for x in ins]
+            if any(x is not None and x.dtype != torch.float64 for x in ins):
                 raise SpmlError(1, name, "device arrays must be float64")
             outs = [torch.empty(oshape, dtype=torch.float64, device=x0.device) for _ in range(nout)]
             self._set_torch_stream(x0)
-            st = getattr(lib, name + "_dev")(self._h, *(_VP(x.data_ptr()) for x in ins), nb,
+            st = getattr(lib, name + "_dev")(self._h, *(_VP(None if x is None else x.data_ptr()) for x in ins), nb,
                                              *(_VP(o.data_ptr()) for o in outs))
         else:
-            ins = [np.ascontiguousarray(x, dtype=np.float64) for x in ins]
+            ins = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in ins]
             outs = [np.empty(oshape) for _ in range(nout)]
-            st = getattr(lib, name)(self._h, *(_VP(x.ctypes.data) for x in ins), nb,
+            st = getattr(lib, name)(self._h, *(_VP(None if x is None else x.ctypes.data) for x in ins), nb,
                                     *(_VP(o.ctypes.data) for o in outs))
         _check(st, name)
         if not batched:
@@ -384,6 +385,15 @@ class SpmlUtil:
     def calc_UVCosLat2VorDiv(self, xy_UCosLat, xy_VCosLat):
         """-> (w_Vor, w_Div) (SpmlUtil_mod.f90:299-314, 342-368)."""
         return self._run("sht_uvcoslat2vordiv", [xy_UCosLat, xy_VCosLat], "spec", nout=2)
+
+    def calc_UVCosLat2VorDiv_fma(self, xy_X1, xy_X2, xy_Q, xy_Z1=None, xy_Z2=None):
+        """calc_UVCosLat2VorDiv(cos(phi) (X1 Q + Z1), cos(phi) (X2 Q + Z2))
+        -> (w_Vor, w_Div), the momentum products formed inside the longitude
+        transform (HBEBaroc_hspm_vfvm_mod.f90:394-418: Q the vorticity, X1, X2
+        the velocities, Z1, Z2 the other terms; both Z or neither)."""
+        if (xy_Z1 is None) != (xy_Z2 is None):
+            raise SpmlError(1, "sht_uvcoslat2vordiv_fma", "Z1 and Z2 must be both given or both None")
+        return self._run("sht_uvcoslat2vordiv_fma", [xy_X1, xy_X2, xy_Q, xy_Z1, xy_Z2], "spec", nout=2)
 
     def calc_VorDiv2UV(self, w_Vor, w_Div):
         """-> (xy_U, xy_V) (SpmlUtil_mod.f90:316-340, 370-396)."""

@@ -58,9 +58,10 @@ extern "C" {
 /* precision modes of the Legendre contraction */
 #define SHT_PREC_FP64  0  /* FP64 operands and FP64 products (the FP64 tensor
                              path, mma.sync f64), FP64 accumulation            */
-#define SHT_PREC_SPLIT 1  /* FP64 operands as six signed 8-bit digits, exact
-                             integer digit products on the tcgen05 tensor
-                             cores, FP64 recombination                         */
+#define SHT_PREC_SPLIT 1  /* FP64 operands as signed 8-bit digits (eight per
+                             grid or spectral value, seven per table value),
+                             exact integer digit products on the tcgen05
+                             tensor cores, FP64 recombination                  */
 
 typedef struct sht_plan_s sht_plan;
 
@@ -72,7 +73,9 @@ SHT_API const char *sht_last_error(void);
 
 /* SpmlUtil_Init(iMax, jMax, kMax, nMax, tMax, RPlanet, np)
  * (SpmlUtil_mod.f90:192-241; wa_Initial at :218-223).
- * im: longitudes (a power of two, 16..2048), or 1 for the axisymmetric model
+ * im: longitudes (even, 16..2048: powers of two take the four-step FFT, other
+ * counts such as 96, 192, 320 or 640 a direct summation over longitudes),
+ * or 1 for the axisymmetric model
  * (DOGCM_MODE_AXISYM, SpmlUtil_mod.f90:30-35,210-211: SPMODEL
  * wa_zonal_module, only the m = 0 modes, lm = nm + 1 with wa(n+1) = a_n^0);
  * jm: Gauss latitudes (even); km: levels (the default batch; informational);
@@ -216,6 +219,19 @@ SHT_API int sht_xya_fluxdiv_xya(sht_plan *plan, const double *xya_a, const doubl
 SHT_API int sht_uvcoslat2vordiv(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
                         int nb, double *wa_vor, double *wa_div);
 
+/* calc_UVCosLat2VorDiv(A, B) of the momentum products
+ *   A = cos(phi) (x1 q + z1),  B = cos(phi) (x2 q + z2),
+ * formed while the grids load: the xy_A, xy_B of HBEBaroc_MOMRHS_VorDivForm
+ * (dynamics/hspm_vfvm/HBEBaroc_hspm_vfvm_mod.f90:394-418; q the vorticity,
+ * x1, x2 the velocities, z1, z2 every other term), whose -w_AlphaOptr_xy(A, B)
+ * and w_AlphaOptr_xy(B, -A) of :430-434 are (-wa_div, wa_vor) here.  Five
+ * grids read once instead of A and B written and read.  z1 and z2 are both
+ * given or both NULL (products only).  SpmlUtil_mod.f90:342-368 for the
+ * transform itself. */
+SHT_API int sht_uvcoslat2vordiv_fma(sht_plan *plan, const double *xya_x1, const double *xya_x2,
+                            const double *xya_q, const double *xya_z1, const double *xya_z2,
+                            int nb, double *wa_vor, double *wa_div);
+
 /* calc_VorDiv2UV: psi = a^2 LaplaInv(Vor), chi = a^2 LaplaInv(Div),
  * U = cos * AlphaOptr(chi, -psi), V = cos * AlphaOptr(psi, chi)
  * (SpmlUtil_mod.f90:316-340, 370-396). */
@@ -265,6 +281,9 @@ SHT_API int sht_xya_fluxdiv_xya_dev(sht_plan *plan, const double *xya_a, const d
                             double *xya);
 SHT_API int sht_uvcoslat2vordiv_dev(sht_plan *plan, const double *xya_ucos, const double *xya_vcos,
                             int nb, double *wa_vor, double *wa_div);
+SHT_API int sht_uvcoslat2vordiv_fma_dev(sht_plan *plan, const double *xya_x1, const double *xya_x2,
+                                const double *xya_q, const double *xya_z1, const double *xya_z2,
+                                int nb, double *wa_vor, double *wa_div);
 SHT_API int sht_vordiv2uv_dev(sht_plan *plan, const double *wa_vor, const double *wa_div,
                       int nb, double *xya_u, double *xya_v);
 SHT_API int sht_wa_lapla_wa_dev(sht_plan *plan, const double *wa, int nb, double *out);

@@ -78,6 +78,87 @@ def test_momrhs_vordiv_batched_vs_oracle_and_per_level(t42):
     assert relerr(vl.cpu().numpy(), v.cpu().numpy()) < 1e-13
 
 
+def test_momrhs_vordiv_fma_vs_oracle(t42):
+    """Products formed in the load: A = cos(phi)(Vor U + za), B = cos(phi)(Vor V + zb)."""
+    sp, ora = t42
+    C = callers()
+    K = 12
+    u, v, vor, za, zb, c = _grids(K, sp.jm, sp.im, 6, seed=4)
+    cs = np.cos(sp.y_Lat)[None, :, None]
+    a, b = cs * (vor * u + za), cs * (vor * v + zb)
+    vor_rhs = -ora.wa_alphaoptr_xya(a, b)
+    div_rhs = ora.wa_alphaoptr_xya(b, -a) - ora.wa_lapla_wa(ora.wa_xya(c))
+    ur, vr = ora.vordiv2uv(vor_rhs, div_rhs)
+    d = [torch.from_numpy(x).cuda() for x in (u, v, vor, za, zb, c)]
+    gu, gv = C.momrhs_vordiv_fma(sp, *d)
+    torch.cuda.synchronize()
+    assert relerr(gu.cpu().numpy(), ur) < TOL and relerr(gv.cpu().numpy(), vr) < TOL
+
+
+@pytest.mark.parametrize("where", ["host", "device"])
+@pytest.mark.parametrize("with_sums", [True, False])
+def test_uvcoslat2vordiv_fma_vs_oracle(t42, where, with_sums):
+    """The fused entry point against calc_UVCosLat2VorDiv of the products, both
+    array kinds, with and without the added terms."""
+    sp, ora = t42
+    u, v, q, za, zb = _grids(5, sp.jm, sp.im, 5, seed=5)
+    if not with_sums:
+        za = zb = None
+    cs = np.cos(sp.y_Lat)[None, :, None]
+    a = cs * (u * q + (za if with_sums else 0.0))
+    b = cs * (v * q + (zb if with_sums else 0.0))
+    rv, rd = ora.uvcoslat2vordiv(a, b)
+    xs = [u, v, q, za, zb]
+    if where == "device":
+        xs = [None if x is None else torch.from_numpy(x).cuda() for x in xs]
+    gv, gd = sp.calc_UVCosLat2VorDiv_fma(*xs)
+    if where == "device":
+        torch.cuda.synchronize()
+        gv, gd = gv.cpu().numpy(), gd.cpu().numpy()
+    assert relerr(gv, rv) < TOL and relerr(gd, rd) < TOL
+
+
+def test_uvcoslat2vordiv_fma_split_and_zonal():
+    """Split precision at T42, and the zonal plan (im = 1) against a 3-D oracle
+    plan of longitude-constant grids (its m = 0 coefficients)."""
+    P, W = pkg(), workloads()
+    I, J, N = W.GRIDS["T42"]
+    sp = P.SpmlUtil(I, J, 1, N, None, A)
+    ora = O.OraclePlan(I, J, N, A)
+    try:
+        sp.set_precision(P.SHT_PREC_SPLIT)
+        u, v, q, za, zb = _grids(6, J, I, 5, seed=6)
+        cs = np.cos(sp.y_Lat)[None, :, None]
+        rv, rd = ora.uvcoslat2vordiv(cs * (u * q + za), cs * (v * q + zb))
+        gv, gd = sp.calc_UVCosLat2VorDiv_fma(*(torch.from_numpy(x).cuda() for x in (u, v, q, za, zb)))
+        torch.cuda.synchronize()
+        assert relerr(gv.cpu().numpy(), rv) < TOL and relerr(gd.cpu().numpy(), rd) < TOL
+    finally:
+        sp.final()
+    z = P.SpmlUtil(1, 64, 1, -1, None, A)
+    try:
+        io = 16
+        while io < 2 * z.nm + 2:
+            io *= 2
+        full = O.OraclePlan(io, 64, z.nm, A)
+        u, v, q, za, zb = _grids(7, 64, 1, 5, seed=8)
+        cs = np.cos(z.y_Lat)[None, :, None]
+        rep = lambda x: np.repeat(x, io, axis=2)
+        rv, rd = full.uvcoslat2vordiv(rep(cs * (u * q + za)), rep(cs * (v * q + zb)))
+        n = np.arange(z.nm + 1)
+        gv, gd = z.calc_UVCosLat2VorDiv_fma(u, v, q, za, zb)
+        assert relerr(gv, rv[:, n * (n + 1)]) < TOL and relerr(gd, rd[:, n * (n + 1)]) < TOL
+    finally:
+        z.final()
+
+
+def test_uvcoslat2vordiv_fma_rejects_one_sum(t42):
+    sp, _ = t42
+    u, v, q, za = _grids(2, sp.jm, sp.im, 4, seed=7)
+    with pytest.raises(pkg().SpmlError):
+        sp.calc_UVCosLat2VorDiv_fma(u, v, q, za, None)
+
+
 def test_diagnose_vordiv_batched_vs_oracle_and_per_level(t42):
     sp, ora = t42
     C = callers()

@@ -281,3 +281,46 @@ def test_legendre_kernel_variants_agree(grid, plans):
     if N <= 170:
         assert relerr(out[3][0], ora.xya_wa(w)) < TOL
         assert relerr(out[3][1], ora.wa_xya(x)) < TOL
+
+
+@pytest.mark.parametrize("grid", [(96, 48, 31), (192, 96, 63), (320, 160, 106)])
+@pytest.mark.parametrize("prec", ["fp64", "split"])
+def test_longitude_counts_with_factors_3_and_5(grid, prec, plans):
+    """im = 96, 192 and 320 (2^5 x 3, 2^6 x 3, 2^6 x 5): dogcm derives
+    nm = (im - 1)/3 from any im (DOGCM_GaussSpmVFvmGrid_mod.f90:209-211), so
+    these grids take the direct longitude transform; every operator against
+    the oracle in both precisions."""
+    P = pkg()
+    I, J, N = grid
+    a = 6.371e6
+    gpu, ora = plans(I, J, N, a)
+    w, w2, x = _inputs(I, J, N, 6, seed=21)
+    gpu.set_precision(P.SHT_PREC_SPLIT if prec == "split" else P.SHT_PREC_FP64)
+    try:
+        assert relerr(gpu.xya_wa(w), ora.xya_wa(w)) < TOL
+        assert relerr(gpu.wa_xya(x), ora.wa_xya(x)) < TOL
+        assert relerr(gpu.xya_GradLon_wa(w), ora.xya_gradlon_wa(w)) < TOL
+        assert relerr(gpu.xya_GradLat_wa(w), ora.xya_gradlat_wa(w)) < TOL
+        u, v = gpu.calc_VorDiv2UV(w / a, w2 / a)
+        uo, vo = ora.vordiv2uv(w / a, w2 / a)
+        assert relerr(u, uo) < TOL and relerr(v, vo) < TOL
+        cs = np.cos(gpu.y_Lat)[None, :, None]
+        vg, dg = gpu.calc_UVCosLat2VorDiv(u * cs, v * cs)
+        vr, dr = ora.uvcoslat2vordiv(u * cs, v * cs)
+        assert relerr(vg, vr) < TOL and relerr(dg, dr) < TOL
+        gpu.synchronize()
+    finally:
+        gpu.set_precision(P.SHT_PREC_FP64)
+
+
+def test_default_truncation_of_a_factor_3_grid():
+    """nm = -1 picks the model's default truncation (im - 1)/3 on a
+    96-longitude grid, and the round trip of band-limited spectra holds."""
+    P, W = pkg(), workloads()
+    gpu = P.SpmlUtil(96, 48, 1, -1)
+    try:
+        assert gpu.nm == 31
+        w = W.seeded_spectra(31, 4, 2.0, seed=3)
+        assert relerr(gpu.wa_xya(gpu.xya_wa(w)), w) < TOL
+    finally:
+        gpu.final()
