@@ -62,6 +62,42 @@ __device__ __forceinline__ double2 cmulc(double2 a, double2 b)  // a * conj(b)
   return make_double2(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
 }
 
+// a e^{-2 pi i t / 32} for a t known at compile time (after unrolling)
+__device__ __forceinline__ double2 rot32(double2 a, int t)
+{
+  if (t == 0) return a;
+  if (t == 8) return make_double2(a.y, -a.x);
+  const double c = cos32(t), s = sin32(t);
+  return make_double2(a.x * c + a.y * s, a.y * c - a.x * s);
+}
+
+// The twiddles of thread column u.  Pass A: W^{u k1} (W = e^{-2 pi i / NC})
+// from the table entries k1 = 1, 2, 3 and k1 = 4, 8, ...: W^{u k1} =
+// W^{u (k1 mod 4)} W^{u 4 (k1 div 4)}, at most one product, 3 + R1/4 - 1
+// shared-memory reads instead of R1 - 1.  Real (un)pack: e^{-2 pi i m / I} for
+// m = u + T q is e^{-2 pi i u / I} e^{-2 pi i q / (2 R1)}, the second factor a
+// constant of the unrolled loop (R1 <= 16), so one read per tile instead of R1.
+// Each value is a product of two correctly rounded factors.
+template <int R1, int T>
+struct PassTwiddles {
+  static constexpr int NB = R1 / 4 > 1 ? R1 / 4 : 1;
+  double2 ta[4], tb[NB];
+  __device__ __forceinline__ void load(const double2 *stw, int u)
+  {
+#pragma unroll
+    for (int t = 1; t < 4 && t < R1; ++t) ta[t] = stw[t * T + u];
+#pragma unroll
+    for (int s = 1; s < NB; ++s) tb[s] = stw[4 * s * T + u];
+  }
+  __device__ __forceinline__ double2 operator()(int k1) const  // k1 >= 1, known at compile time
+  {
+    const int t = k1 & 3, s = k1 >> 2;
+    if (s == 0) return ta[t];
+    if (t == 0) return tb[s];
+    return cmul(ta[t], tb[s]);
+  }
+};
+
 // In-register radix-2 decimation-in-frequency DFT of size 2^LOG (<= 32),
 // sign -1 (forward) or +1 (INV).  Output is left in bit-reversed order:
 // X[k] = v[brev<LOG>(k)].
@@ -192,10 +228,12 @@ __device__ __forceinline__ void fwd_tile(const FftArgs &a, double2 (&v)[1 << A],
   const long long mstride = (long long)a.ncolF * a.J;
   dft_reg<A, false>(v);
   double2 *srow = cur + r * RS;
+  PassTwiddles<R1, T> tw;
+  tw.load(stw, u);
 #pragma unroll
   for (int k1 = 0; k1 < R1; ++k1) {
     double2 y = v[brev<A>(k1)];
-    if (k1 != 0) y = cmul(y, stw[k1 * T + u]);
+    if (k1 != 0) y = cmul(y, tw(k1));
     srow[u * (R1 + 1) + k1] = y;
   }
   __syncthreads();
@@ -219,6 +257,7 @@ __device__ __forceinline__ void fwd_tile(const FftArgs &a, double2 (&v)[1 << A],
   // real unpack: X_m = E - i W^m D, E/D = (Z_m +- conj Z_{NC-m})/2, W = e^{-2 pi i/I},
   // written transposed (m-major) for the output runs
   const double sc = valid ? __ldg(a.rowscale + j) : 0.0;
+  const double2 cu = stwI[u];
 #pragma unroll
   for (int q = 0; q < R1; ++q) {
     const int s = q % NS, k2 = q / NS, m = u + T * q;
@@ -231,7 +270,7 @@ __device__ __forceinline__ void fwd_tile(const FftArgs &a, double2 (&v)[1 << A],
       const double2 zm = z[s][brev<B>(k2)];
       const double er = 0.5 * (zm.x + zc.x), ei = 0.5 * (zm.y - zc.y);
       const double dr = 0.5 * (zm.x - zc.x), di = 0.5 * (zm.y + zc.y);
-      const double2 w = stwI[m];
+      const double2 w = R1 <= 16 ? rot32(cu, q * (16 / R1)) : stwI[m];  // e^{-2 pi i m / I}
       const double tr = w.x * dr - w.y * di, ti = w.x * di + w.y * dr;
       cur[m * JTp + r] = make_double2((er + ti) * sc, (m == 0) ? 0.0 : (ei - tr) * sc);
     }
@@ -441,6 +480,7 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
       }
     }
     const int lane = tid & 31, partner = (lane & ~(T - 1)) | ((T - u) & (T - 1));
+    const double2 cu = stwI[u];
     double2 v[R1];
 #pragma unroll
     for (int n1 = 0; n1 < R1; ++n1) {
@@ -464,7 +504,7 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
           Y = make_double2(q.x, -q.y);
         }
       }
-      const double2 wI = stwI[k];
+      const double2 wI = kShfl ? rot32(cu, n1 * (16 / R1)) : stwI[k];  // e^{-2 pi i k / I}
       const double wr = wI.x, wi = -wI.y;
       const double dr = X.x - Y.x, di = X.y - Y.y;
       const double tr = wr * dr - wi * di, ti = wr * di + wi * dr;
@@ -488,10 +528,12 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
 
     dft_reg<A, true>(v);
     double2 *srow = cur + r * RS;
+    PassTwiddles<R1, T> tw;
+    tw.load(stw, u);
 #pragma unroll
     for (int k1 = 0; k1 < R1; ++k1) {
       double2 y = v[brev<A>(k1)];
-      if (k1 != 0) y = cmulc(y, stw[k1 * T + u]);
+      if (k1 != 0) y = cmulc(y, tw(k1));
       srow[u * (R1 + 1) + k1] = y;
     }
     __syncthreads();

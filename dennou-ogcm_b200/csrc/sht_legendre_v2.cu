@@ -176,6 +176,11 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
       const double *G = Gcur + mi * ct_fwd(JH) * g.CS + (par ? 2 * JH : 0);
       const int r0 = par + 2 * (16 * gi + (lane >> 2));
       const int r1 = r0 + 16;
+      // the job's second 8-row tile holds rows of this parity only when the
+      // parity has more than 16 gi + 8 of them; otherwise its products are
+      // skipped (an eighth to a quarter of the tiles at T42-T85)
+      const int cnt = par ? R / 2 : (R + 1) / 2;
+      const bool two = 16 * gi + 8 < cnt;
       // K order within each pair of k-steps: lane q = lane & 3 takes latitude
       // 8j + 2q in the first and 8j + 2q + 1 in the second, so one 16-byte
       // load gives a lane both A values.  The columns form four 8-column
@@ -193,22 +198,38 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
         for (int h = 0; h < NH; ++h)
 #pragma unroll
           for (int pt = 0; pt < 2; ++pt) acc[t][h][pt][0] = acc[t][h][pt][1] = 0.0;
+      if (two) {
 #pragma unroll
-      for (int kb = 0; kb < JH; kb += 8) {
-        const double2 a0 = *reinterpret_cast<const double2 *>(pa0 + kb);
-        const double2 a1 = *reinterpret_cast<const double2 *>(pa1 + kb);
+        for (int kb = 0; kb < JH; kb += 8) {
+          const double2 a0 = *reinterpret_cast<const double2 *>(pa0 + kb);
+          const double2 a1 = *reinterpret_cast<const double2 *>(pa1 + kb);
 #pragma unroll
-        for (int h = 0; h < NH; ++h) {
-          const double2 be = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb);      // latitude 8j + 2q
-          const double2 bo = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb + 2);  // latitude 8j + 2q + 1
-          mma884(acc[0][h][0], a0.x, be.x);
-          mma884(acc[0][h][1], a0.x, be.y);
-          mma884(acc[1][h][0], a1.x, be.x);
-          mma884(acc[1][h][1], a1.x, be.y);
-          mma884(acc[0][h][0], a0.y, bo.x);
-          mma884(acc[0][h][1], a0.y, bo.y);
-          mma884(acc[1][h][0], a1.y, bo.x);
-          mma884(acc[1][h][1], a1.y, bo.y);
+          for (int h = 0; h < NH; ++h) {
+            const double2 be = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb);      // latitude 8j + 2q
+            const double2 bo = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb + 2);  // latitude 8j + 2q + 1
+            mma884(acc[0][h][0], a0.x, be.x);
+            mma884(acc[0][h][1], a0.x, be.y);
+            mma884(acc[1][h][0], a1.x, be.x);
+            mma884(acc[1][h][1], a1.x, be.y);
+            mma884(acc[0][h][0], a0.y, bo.x);
+            mma884(acc[0][h][1], a0.y, bo.y);
+            mma884(acc[1][h][0], a1.y, bo.x);
+            mma884(acc[1][h][1], a1.y, bo.y);
+          }
+        }
+      } else {
+#pragma unroll
+        for (int kb = 0; kb < JH; kb += 8) {
+          const double2 a0 = *reinterpret_cast<const double2 *>(pa0 + kb);
+#pragma unroll
+          for (int h = 0; h < NH; ++h) {
+            const double2 be = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb);
+            const double2 bo = *reinterpret_cast<const double2 *>(gb + 8 * h * g.CS + 2 * kb + 2);
+            mma884(acc[0][h][0], a0.x, be.x);
+            mma884(acc[0][h][1], a0.x, be.y);
+            mma884(acc[0][h][0], a0.y, bo.x);
+            mma884(acc[0][h][1], a0.y, bo.y);
+          }
         }
       }
       const long long rowbase = a.rowoff[m];
