@@ -388,7 +388,9 @@ int host_graph_call(sht_plan *p, int op, int nb, Enqueue &&enqueue)
   }
   HostGraph *g = nullptr;
   for (HostGraph &c : gs)
-    if (c.op == op && c.nb == nb && c.precision == p->precision && c.leg_kernel == p->leg_kernel) g = &c;
+    if (c.op == op && c.nb == nb && c.precision == p->precision && c.leg_kernel == p->leg_kernel &&
+        c.leg_tile == p->leg_tile)
+      g = &c;
   cudaError_t e;
   if (g && g->exec) {
     if ((e = cudaGraphLaunch(g->exec, s)) != cudaSuccess) return cuda_fail(e, "graph launch");
@@ -402,7 +404,8 @@ int host_graph_call(sht_plan *p, int op, int nb, Enqueue &&enqueue)
         gs.erase(gs.begin());
       }
       HostGraph n;
-      n.op = op; n.nb = nb; n.precision = p->precision; n.leg_kernel = p->leg_kernel; n.gen = p->buf_gen;
+      n.op = op; n.nb = nb; n.precision = p->precision; n.leg_kernel = p->leg_kernel; n.leg_tile = p->leg_tile;
+      n.gen = p->buf_gen;
       gs.push_back(n);
     }
     return enqueue(s);
@@ -434,7 +437,9 @@ int host_graph_call(sht_plan *p, int op, int nb, Enqueue &&enqueue)
   // g may have moved if the list changed; find the entry again
   g = nullptr;
   for (HostGraph &c : gs)
-    if (c.op == op && c.nb == nb && c.precision == p->precision && c.leg_kernel == p->leg_kernel) g = &c;
+    if (c.op == op && c.nb == nb && c.precision == p->precision && c.leg_kernel == p->leg_kernel &&
+        c.leg_tile == p->leg_tile)
+      g = &c;
   if (rc != SHT_OK || e != cudaSuccess || !exec) {
     cudaGetLastError();
     if (exec) cudaGraphExecDestroy(exec);
@@ -922,6 +927,13 @@ int sht_set_option(sht_plan *p, int option, int value)
     if (value < 0 || value > 3) { set_error("legendre kernel option must be 0, 1, 2 or 3"); return SHT_ERR_INVALID_ARG; }
     p->leg_kernel = value;
     return SHT_OK;
+  case SHT_OPT_LEGENDRE_TILE:
+    if (value != 0 && value != 8 && value != 16 && value != 32) {
+      set_error("legendre tile option must be 0, 8, 16 or 32");
+      return SHT_ERR_INVALID_ARG;
+    }
+    p->leg_tile = value;
+    return SHT_OK;
   case SHT_OPT_HOST_GRAPHS:
     if (value != 0 && value != 1) { set_error("host graphs option must be 0 or 1"); return SHT_ERR_INVALID_ARG; }
     p->host_graphs = value == 1;
@@ -937,6 +949,7 @@ int sht_get_option(const sht_plan *p, int option, int *value)
   if (!value) { set_error("NULL output"); return SHT_ERR_INVALID_ARG; }
   switch (option) {
   case SHT_OPT_LEGENDRE_KERNEL: *value = p->leg_kernel; return SHT_OK;
+  case SHT_OPT_LEGENDRE_TILE: *value = p->leg_tile; return SHT_OK;
   case SHT_OPT_HOST_GRAPHS: *value = p->host_graphs ? 1 : 0; return SHT_OK;
   case SHT_OPT_HOST_GRAPH_COUNT: {
     std::lock_guard<std::mutex> lk(const_cast<sht_plan *>(p)->mtx);

@@ -65,7 +65,7 @@ struct Timing {
 // Every pointer in it is a plan buffer, so it replays for any caller arrays
 // of the same operator and size until a buffer is reallocated (buf_gen).
 struct HostGraph {
-  int op = -1, nb = 0, precision = 0, leg_kernel = 0;
+  int op = -1, nb = 0, precision = 0, leg_kernel = 0, leg_tile = 0;
   unsigned long long gen = 0;
   cudaGraphExec_t exec = nullptr;  // null after the first call, or when not capturable
   bool failed = false;             // capture was refused: run this call uncaptured
@@ -92,6 +92,7 @@ struct sht_plan_s {
   int M = 0;           // orders transformed: N + 1, or 1 for a zonal plan
   int precision = SHT_PREC_FP64;
   int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent
+  int leg_tile = 0;    // SHT_OPT_LEGENDRE_TILE: 0 auto; paired kernels: analysis columns per item (8, 16); chunked kernels: latitudes per chunk (16, 32)
 
   // device tables
   double *d_mu = nullptr, *d_wgt = nullptr, *d_rowscale = nullptr;

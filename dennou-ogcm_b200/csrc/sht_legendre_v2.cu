@@ -38,7 +38,8 @@ constexpr int kW = 8;            // warps per block
 constexpr int kT = kW * 32;      // threads per block
 constexpr int kCT = 16;          // complex columns per item (synthesis)
 // complex columns per analysis item: 8 at JH = 64 (one panel per block, two
-// blocks per SM), 16 below, where an item's contraction is short
+// blocks per SM), 16 below, where an item's contraction is short; the plan's
+// SHT_OPT_LEGENDRE_TILE (8 or 16) overrides it where the panel fits
 __host__ __device__ constexpr int ct_fwd(int JH) { return JH >= 64 ? 8 : 16; }
 
 struct Geo {
@@ -102,11 +103,10 @@ __device__ void load_pair_P(const V2Args &a, const Geo &g, double *Pbuf, int ma,
 
 // ------------------------------------------------------------------ analysis
 // Thread q copies latitude (q mod J) of column rows q/J, q/J + kT/J, ...
-template <int JH>
+template <int JH, int CT>
 __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma, int mb, int col0)
 {
   constexpr int J = 2 * JH, RSTEP = kT / J;  // column rows covered per pass
-  constexpr int CT = ct_fwd(JH);
   const int nrow = (mb >= 0) ? 2 * CT : CT;
   const int j = threadIdx.x % J;
 #pragma unroll 4
@@ -119,7 +119,7 @@ __device__ void load_F_panels(const V2Args &a, const Geo &g, double *buf, int ma
   }
 }
 
-template <int JH>
+template <int JH, int CT>
 __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
 {
   // One data panel per block and two blocks per SM: each block's panel load
@@ -135,13 +135,13 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
 
   int cur = -1;
   for (int it = it0; it < it1; ++it) {
-    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * ct_fwd(JH);
+    const int pidx = it / a.ntiles, col0 = (it - pidx * a.ntiles) * CT;
     const int2 pr = a.pairs[pidx];
     if (pidx != cur) {
       load_pair_P<JH>(a, g, Pbuf, pr.x, pr.y);
       cur = pidx;
     }
-    load_F_panels<JH>(a, g, G0, pr.x, pr.y, col0);
+    load_F_panels<JH, CT>(a, g, G0, pr.x, pr.y, col0);
     cp_commit();
     cp_wait0();
     __syncthreads();
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
       // The panel's Fourier lines are in shared memory now and no later kernel
       // reads them: drop them from L2 without a write-back.  A column row is
       // J complex values, a whole number of 128-byte lines.
-      constexpr int CT = ct_fwd(JH), LPR = 2 * JH * 16 / 128;
+      constexpr int LPR = 2 * JH * 16 / 128;
       const int nrow = (pr.y >= 0) ? 2 * CT : CT;
       for (int q = threadIdx.x; q < nrow * LPR; q += kT) {
         const int row = q / LPR, b = row % CT, m = (row / CT) ? pr.y : pr.x;
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
       else { mi = 1; par = 1; gi = job - gEa - gOa - gEb; }
       const int m = mi ? pr.y : pr.x, R = mi ? Rb : Ra;
       const double *Pm = Pbuf + (mi ? Ra : 0) * g.PS;
-      const double *G = Gcur + mi * ct_fwd(JH) * g.CS + (par ? 2 * JH : 0);
+      const double *G = Gcur + mi * CT * g.CS + (par ? 2 * JH : 0);
       const int r0 = par + 2 * (16 * gi + (lane >> 2));
       const int r1 = r0 + 16;
       // the job's second 8-row tile holds rows of this parity only when the
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kT, 2) k_leg_fwd_pair(V2Args a)
       const double *pa0 = Pm + min(r0, R - 1) * g.PS + 2 * q;
       const double *pa1 = Pm + min(r1, R - 1) * g.PS + 2 * q;
       const double *gb = G + (lane >> 2) * g.CS + 4 * q;
-      constexpr int NH = ct_fwd(JH) / 8;
+      constexpr int NH = CT / 8;
       double acc[2][NH][2][2];  // [row tile][colrow half][re/im][2 columns]
 #pragma unroll
       for (int t = 0; t < 2; ++t)
@@ -388,10 +388,18 @@ __global__ void __launch_bounds__(kT, 1) k_leg_inv_pair(V2Args a)
   cp_wait0();
 }
 
-size_t fwd_smem(int N, int J)
+size_t fwd_smem(int N, int J, int ct)
 {
   const Geo g = make_geo(N, J, true);
-  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * ct_fwd(J / 2) * (size_t)g.CS);
+  return sizeof(double) * ((size_t)g.prow_cap * g.PS + 2 * ct * (size_t)g.CS);
+}
+
+// analysis columns per item: the plan's tile choice when its panel fits
+int fwd_ct(const sht_plan *p)
+{
+  const int t = p->leg_tile;
+  if ((t == 8 || t == 16) && fwd_smem(p->N, p->J, t) <= 227 * 1024) return t;
+  return ct_fwd(p->JH);
 }
 size_t inv_smem(int N, int J)
 {
@@ -416,15 +424,21 @@ int launch_pair(const sht_plan *p, bool inverse, const double2 *in, int ncol, do
   int npairs = 0;
   int rc = get_pairs(p, &a.pairs, &npairs);
   if (rc) { set_error("legendre: pair table missing"); return rc; }
-  const int ct = inverse ? kCT : ct_fwd(p->JH);
+  const int ct = inverse ? kCT : fwd_ct(p);
   a.ntiles = (ncol + ct - 1) / ct;
   a.nitems = npairs * a.ntiles;
-  const size_t smem = inverse ? inv_smem(p->N, p->J) : fwd_smem(p->N, p->J);
+  const size_t smem = inverse ? inv_smem(p->N, p->J) : fwd_smem(p->N, p->J, ct);
   void (*kern)(V2Args) = nullptr;
-  switch (p->JH) {
-  case 16: kern = inverse ? k_leg_inv_pair<16> : k_leg_fwd_pair<16>; break;
-  case 32: kern = inverse ? k_leg_inv_pair<32> : k_leg_fwd_pair<32>; break;
-  case 64: kern = inverse ? k_leg_inv_pair<64> : k_leg_fwd_pair<64>; break;
+  switch (p->JH * 100 + (inverse ? 0 : ct)) {
+  case 1600: case 3200: case 6400:
+    kern = p->JH == 16 ? k_leg_inv_pair<16> : p->JH == 32 ? k_leg_inv_pair<32> : k_leg_inv_pair<64>;
+    break;
+  case 1608: kern = k_leg_fwd_pair<16, 8>; break;
+  case 1616: kern = k_leg_fwd_pair<16, 16>; break;
+  case 3208: kern = k_leg_fwd_pair<32, 8>; break;
+  case 3216: kern = k_leg_fwd_pair<32, 16>; break;
+  case 6408: kern = k_leg_fwd_pair<64, 8>; break;
+  case 6416: kern = k_leg_fwd_pair<64, 16>; break;
   default: set_error("legendre: latitude count outside the paired kernels"); return SHT_ERR_UNSUPPORTED_SIZE;
   }
   int per_sm = 0;
@@ -445,7 +459,7 @@ bool leg_pair_supported(const sht_plan *p)
 {
   if (p->J % 16 != 0 || (p->JH != 16 && p->JH != 32 && p->JH != 64)) return false;
   const size_t lim = 227 * 1024;
-  return fwd_smem(p->N, p->J) <= lim && inv_smem(p->N, p->J) <= lim;
+  return fwd_smem(p->N, p->J, ct_fwd(p->JH)) <= lim && inv_smem(p->N, p->J) <= lim;
 }
 
 int launch_leg_fwd_pair(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)

@@ -367,11 +367,13 @@ int max_jobs(int N)
   return best;
 }
 
-bool choose(const sht_plan *p, Choice *c)
+bool choose_tile(const sht_plan *p, int want, Choice *c)
 {
   const size_t lim = 227 * 1024;
   if (p->JH % 32 != 0) return false;
-  c->KC = (p->JH <= 128) ? 32 : 16;
+  // latitudes per chunk: 32 up to JH = 128, 16 above; the plan's
+  // SHT_OPT_LEGENDRE_TILE (16 or 32) overrides it where the stages fit
+  c->KC = (want == 16 || want == 32) ? want : (p->JH <= 128) ? 32 : 16;
   c->KL = c->KC;
   const int jobs = max_jobs(p->N);
   c->JPW = (jobs + kW - 1) / kW;
@@ -384,6 +386,13 @@ bool choose(const sht_plan *p, Choice *c)
   c->DB = sizeof(double) * (2 * pst + 2 * ast) <= lim;
   c->inv_smem = sizeof(double) * (2 * pst + (c->DB ? 2 : 1) * ast);
   return c->fwd_smem <= lim && c->inv_smem <= lim;
+}
+
+// the plan's tile choice, or the automatic one where that does not fit
+bool choose(const sht_plan *p, Choice *c)
+{
+  if (choose_tile(p, p->leg_tile, c)) return true;
+  return p->leg_tile != 0 && choose_tile(p, 0, c);
 }
 
 template <typename K>

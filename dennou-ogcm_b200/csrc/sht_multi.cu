@@ -36,7 +36,7 @@ struct Group {
   const double **d_gcol = nullptr;  // ncol grid column pointers (device)
   double **d_wcol = nullptr;        // ncol spectral column pointers (device)
   double2 *F = nullptr, *S = nullptr;
-  int precision = SHT_PREC_FP64, leg_kernel = 0;
+  int precision = SHT_PREC_FP64, leg_kernel = 0, leg_tile = 0;
   float tuned_ms = 0.f;
   cudaEvent_t join = nullptr;
 };
@@ -81,13 +81,14 @@ bool live(const sht_multi *m) { return m && m->magic == kMultiMagic; }
 // order) and points each plan at its own stream with the group's Legendre
 // configuration; everything is restored on release.
 struct PlanLease {
-  struct Saved { sht_plan *p; cudaStream_t stream; int precision, leg_kernel; bool timing; };
+  struct Saved { sht_plan *p; cudaStream_t stream; int precision, leg_kernel, leg_tile; bool timing; };
   std::vector<Saved> saved;
   explicit PlanLease(sht_multi *m)
   {
     for (Group &g : m->groups) {
       g.plan->mtx.lock();
-      saved.push_back({g.plan, g.plan->stream, g.plan->precision, g.plan->leg_kernel, g.plan->timing.on});
+      saved.push_back({g.plan, g.plan->stream, g.plan->precision, g.plan->leg_kernel, g.plan->leg_tile,
+                       g.plan->timing.on});
       g.plan->stream = g.plan->own_stream;
       g.plan->timing.on = false;
       apply(g);
@@ -97,6 +98,7 @@ struct PlanLease {
   {
     g.plan->precision = g.precision;
     g.plan->leg_kernel = g.leg_kernel;
+    g.plan->leg_tile = g.leg_tile;
   }
   ~PlanLease()
   {
@@ -104,6 +106,7 @@ struct PlanLease {
       it->p->stream = it->stream;
       it->p->precision = it->precision;
       it->p->leg_kernel = it->leg_kernel;
+      it->p->leg_tile = it->leg_tile;
       it->p->timing.on = it->timing;
       it->p->mtx.unlock();
     }
@@ -177,17 +180,27 @@ int time_group(Group &g, int reps, float *ms)
 
 int tune_group(Group &g, bool allow_split)
 {
-  struct Cand { int precision, leg_kernel; };
+  // kernel families and their tiles: analysis columns per item of the paired
+  // kernels, latitudes per chunk of the chunked kernels (a tile a kernel
+  // cannot take falls back to its automatic one and is timed again harmlessly)
+  struct Cand { int precision, leg_kernel, leg_tile; };
   std::vector<Cand> cands;
-  if (leg_pair_supported(g.plan)) cands.push_back({SHT_PREC_FP64, 2});
-  if (leg_chunk_supported(g.plan)) cands.push_back({SHT_PREC_FP64, 3});
-  cands.push_back({SHT_PREC_FP64, 1});
-  if (allow_split && split_supported(g.plan)) cands.push_back({SHT_PREC_SPLIT, 0});
+  if (leg_pair_supported(g.plan)) {
+    cands.push_back({SHT_PREC_FP64, 2, 8});
+    cands.push_back({SHT_PREC_FP64, 2, 16});
+  }
+  if (leg_chunk_supported(g.plan)) {
+    cands.push_back({SHT_PREC_FP64, 3, 16});
+    cands.push_back({SHT_PREC_FP64, 3, 32});
+  }
+  cands.push_back({SHT_PREC_FP64, 1, 0});
+  if (allow_split && split_supported(g.plan)) cands.push_back({SHT_PREC_SPLIT, 0, 0});
   float best = 0.f;
   Cand win = cands.front();
   for (const Cand &c : cands) {
     g.precision = c.precision;
     g.leg_kernel = c.leg_kernel;
+    g.leg_tile = c.leg_tile;
     PlanLease::apply(g);
     float ms = 0.f;
     int rc = time_group(g, 3, &ms);
@@ -196,6 +209,7 @@ int tune_group(Group &g, bool allow_split)
   }
   g.precision = win.precision;
   g.leg_kernel = win.leg_kernel;
+  g.leg_tile = win.leg_tile;
   g.tuned_ms = best;
   PlanLease::apply(g);
   return SHT_OK;
@@ -250,6 +264,7 @@ int build(sht_multi *m, int flags)
       return cuda_fail(e, "multi column tables");
     G.precision = p->precision;
     G.leg_kernel = p->leg_kernel;
+    G.leg_tile = p->leg_tile;
   }
 
   PlanLease lease(m);
@@ -396,6 +411,16 @@ int sht_multi_group_info(const sht_multi *m, int group, int *ncol, int *precisio
   if (precision) *precision = g.precision;
   if (legendre_kernel) *legendre_kernel = g.leg_kernel;
   if (tuned_ms) *tuned_ms = g.tuned_ms;
+  return SHT_OK;
+}
+
+int sht_multi_group_tile(const sht_multi *m, int group, int *legendre_tile)
+{
+  if (!live(m) || !legendre_tile || group < 0 || group >= (int)m->groups.size()) {
+    set_error("multi: bad group");
+    return SHT_ERR_INVALID_ARG;
+  }
+  *legendre_tile = m->groups[group].leg_tile;
   return SHT_OK;
 }
 

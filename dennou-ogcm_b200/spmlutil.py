@@ -32,6 +32,7 @@ SHT_PREC_SPLIT = 1
 SHT_OPT_LEGENDRE_KERNEL = 1
 SHT_OPT_HOST_GRAPHS = 2
 SHT_OPT_HOST_GRAPH_COUNT = 3
+SHT_OPT_LEGENDRE_TILE = 4
 SHT_MULTI_SYNTHESIS, SHT_MULTI_ANALYSIS, SHT_MULTI_ROUND_TRIP = 1, 2, 3
 SHT_MULTI_AUTOTUNE, SHT_MULTI_ALLOW_SPLIT, SHT_MULTI_NO_GRAPH = 1, 2, 4
 
@@ -122,6 +123,7 @@ def load_library(path: str | None = None):
     lib.sht_multi_groups.argtypes = [_VP, ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_group_info.argtypes = [_VP, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 3 + \
         [ctypes.POINTER(ctypes.c_float)]
+    lib.sht_multi_group_tile.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_kernels.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_destroy.argtypes = [_VP]
     _lib = lib
@@ -576,7 +578,7 @@ class MultiTransform:
         _check(self._lib.sht_multi_set_stream(self._h, stream.cuda_stream), "sht_multi_set_stream")
 
     def groups(self):
-        """Per plan group: dict(ncol, precision, legendre_kernel, tuned_ms)."""
+        """Per plan group: dict(ncol, precision, legendre_kernel, legendre_tile, tuned_ms)."""
         n = ctypes.c_int()
         _check(self._lib.sht_multi_groups(self._h, ctypes.byref(n)), "sht_multi_groups")
         out = []
@@ -584,7 +586,10 @@ class MultiTransform:
             nc, pr, lk, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
             _check(self._lib.sht_multi_group_info(self._h, g, ctypes.byref(nc), ctypes.byref(pr), ctypes.byref(lk),
                                                   ctypes.byref(ms)), "sht_multi_group_info")
-            out.append(dict(ncol=nc.value, precision=pr.value, legendre_kernel=lk.value, tuned_ms=ms.value))
+            tile = ctypes.c_int()
+            _check(self._lib.sht_multi_group_tile(self._h, g, ctypes.byref(tile)), "sht_multi_group_tile")
+            out.append(dict(ncol=nc.value, precision=pr.value, legendre_kernel=lk.value, legendre_tile=tile.value,
+                            tuned_ms=ms.value))
         return out
 
     def kernels(self, what: int = SHT_MULTI_ROUND_TRIP) -> int:

@@ -131,6 +131,14 @@ SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
  * is the number of graphs the plan holds. */
 #define SHT_OPT_HOST_GRAPHS 2
 #define SHT_OPT_HOST_GRAPH_COUNT 3
+/* SHT_OPT_LEGENDRE_TILE: the tile of the FP64 Legendre kernels (0 automatic).
+ * Paired kernels: 8 or 16 complex columns per analysis item; chunked kernels:
+ * 16 or 32 latitudes per streamed chunk.  A value the chosen kernel does not
+ * take, or whose shared memory does not fit, falls back to the automatic
+ * tile.  Results are identical for every tile (the same products in the same
+ * order per output).  The batch tuner (sht_multi_build with autotune) times
+ * the tiles with the kernel families. */
+#define SHT_OPT_LEGENDRE_TILE 4
 SHT_API int sht_set_option(sht_plan *plan, int option, int value);
 SHT_API int sht_get_option(const sht_plan *plan, int option, int *value);
 
@@ -406,6 +414,8 @@ SHT_API int sht_multi_synchronize(sht_multi *multi);
 SHT_API int sht_multi_groups(const sht_multi *multi, int *ngroups);
 SHT_API int sht_multi_group_info(const sht_multi *multi, int group, int *ncol, int *precision,
                                  int *legendre_kernel, float *tuned_ms);
+/* The SHT_OPT_LEGENDRE_TILE value the group runs with (the tuner's choice). */
+SHT_API int sht_multi_group_tile(const sht_multi *multi, int group, int *legendre_tile);
 /* Kernel launches one sht_multi_run(what) replays. */
 SHT_API int sht_multi_kernels(const sht_multi *multi, int what, int *nkernels);
 SHT_API int sht_multi_destroy(sht_multi *multi);

@@ -283,6 +283,38 @@ def test_legendre_kernel_variants_agree(grid, plans):
         assert relerr(out[3][1], ora.wa_xya(x)) < TOL
 
 
+@pytest.mark.parametrize("grid", [(64, 32, 21), (256, 128, 85), (512, 256, 170), (1024, 512, 341)])
+def test_legendre_tiles_agree(grid, plans):
+    """Every tile of the paired kernel (8 or 16 analysis columns per item) and
+    of the chunked kernel (16 or 32 latitudes per chunk) gives the same
+    results bit for bit, and matches the oracle; a tile a kernel cannot take
+    falls back to its automatic one."""
+    P = pkg()
+    I, J, N = grid
+    gpu, ora = plans(I, J, N)
+    nb = 37 if N < 300 else 11
+    w, w2, x = _inputs(I, J, N, nb, seed=23)
+    try:
+        for kern in (2, 3):
+            gpu.set_option(P.SHT_OPT_LEGENDRE_KERNEL, kern)
+            out = {}
+            for tile in (0, 8, 16, 32):
+                gpu.set_option(P.SHT_OPT_LEGENDRE_TILE, tile)
+                assert gpu.get_option(P.SHT_OPT_LEGENDRE_TILE) == tile
+                out[tile] = (gpu.wa_xya(x), gpu.xya_wa(w), gpu.wa_DivMu_xya(x))
+            for tile in (8, 16, 32):
+                for k in range(3):
+                    assert np.array_equal(out[tile][k], out[0][k]), (kern, tile, k)
+            if N <= 170:
+                assert relerr(out[0][0], ora.wa_xya(x)) < TOL
+                assert relerr(out[0][1], ora.xya_wa(w)) < TOL
+        with pytest.raises(P.SpmlError):
+            gpu.set_option(P.SHT_OPT_LEGENDRE_TILE, 12)
+    finally:
+        gpu.set_option(P.SHT_OPT_LEGENDRE_TILE, 0)
+        gpu.set_option(P.SHT_OPT_LEGENDRE_KERNEL, 0)
+
+
 @pytest.mark.parametrize("grid", [(96, 48, 31), (192, 96, 63), (320, 160, 106)])
 @pytest.mark.parametrize("prec", ["fp64", "split"])
 def test_longitude_counts_with_factors_3_and_5(grid, prec, plans):
