@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kThreads) k_leg_inv_dmma(LegArgs a)
     __syncthreads();
 #pragma unroll
     for (int q = 0; q < MAXU; ++q) {
-      const int u = warp + kWarps * q;
+      const int u = warp + kWarps * (q + MAXU * (int)blockIdx.z);
       if (u < nunits) {
         const int g = u / ks, s = u - g * ks;
         const int jh0 = 16 * g;
@@ -288,7 +288,7 @@ __global__ void __launch_bounds__(kThreads) k_leg_inv_dmma(LegArgs a)
   // Ge at F[m][col][jh], Go at F[m][col][JH + jh]
 #pragma unroll
   for (int q = 0; q < MAXU; ++q) {
-    const int u = warp + kWarps * q;
+    const int u = warp + kWarps * (q + MAXU * (int)blockIdx.z);
     if (u >= nunits || (u % ks) != 0) continue;
     const int jh0 = 16 * (u / ks);
 #pragma unroll
@@ -386,10 +386,13 @@ int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *
   const int maxu = (ngj + kWarps - 1) / kWarps;
   dim3 grid((ncol + kCT - 1) / kCT, p->M);
   const size_t smem = inv_smem();
+  // up to two 16-latitude units per warp; beyond that (JH > 256) the units
+  // are split over two blocks (grid z), each staging the coefficient rows
+  // itself, rather than four accumulator sets per warp that spill
   switch (maxu) {
   case 1: return launch(k_leg_inv_dmma<1>, grid, smem, s, a, "k_leg_inv_dmma");
   case 2: return launch(k_leg_inv_dmma<2>, grid, smem, s, a, "k_leg_inv_dmma");
-  case 3: case 4: return launch(k_leg_inv_dmma<4>, grid, smem, s, a, "k_leg_inv_dmma");
+  case 3: case 4: grid.z = 2; return launch(k_leg_inv_dmma<2>, grid, smem, s, a, "k_leg_inv_dmma");
   default: set_error("legendre: too many latitudes"); return SHT_ERR_UNSUPPORTED_SIZE;
   }
 }

@@ -425,10 +425,16 @@ __device__ __forceinline__ void load16(const I8Args &a, const Unit &u, int col, 
 #pragma unroll
     for (int i = 0; i < 16; ++i) x[i] = (cv && k0 + i < u.K) ? src[k0 + i] : make_double2(0.0, 0.0);
   } else {
-    const double2 *src = a.Sc + ((long long)u.rowoff + u.p) * a.ncol + (cv ? col : 0);
+    // one row pointer advanced by two internal rows (one parity) per value:
+    // no per-value 64-bit index products held for the whole batch of loads
+    const size_t step = (size_t)2 * a.ncol;
+    const double2 *src = a.Sc + ((long long)u.rowoff + u.p + 2 * k0) * a.ncol + (cv ? col : 0);
+    const int nv = cv ? u.K - k0 : 0;
 #pragma unroll
-    for (int i = 0; i < 16; ++i)
-      x[i] = (cv && k0 + i < u.K) ? src[(long long)2 * (k0 + i) * a.ncol] : make_double2(0.0, 0.0);
+    for (int i = 0; i < 16; ++i) {
+      x[i] = i < nv ? *src : make_double2(0.0, 0.0);
+      src += step;
+    }
   }
 }
 
@@ -528,19 +534,20 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
       for (int pp = 0; pp < 2; ++pp) {
         const int part = pp ^ first_part;
         const double sc = i8::pow2(i8::kBitsData - (part ? (ps ? ei1 : ei0) : (ps ? er1 : er0)));
-        // all 16 conversions first (independent), then the byte permutes
-        uint32_t lo[16], hi[16];
-#pragma unroll
-        for (int i = 0; i < 16; ++i) {
-          const unsigned long long y = i8::data_word(part ? x[i].y : x[i].x, sc);
-          lo[i] = (uint32_t)y;
-          hi[i] = (uint32_t)(y >> 32);
-        }
+        // four values at a time: conversions, then their byte permutes (the
+        // groups are independent, and fewer words are live at once)
         uint32_t w[4][kDigitsData];
 #pragma unroll
-        for (int g = 0; g < 4; ++g)
-          i8::digit_words_data({lo[4 * g], lo[4 * g + 1], lo[4 * g + 2], lo[4 * g + 3]},
-                               {hi[4 * g], hi[4 * g + 1], hi[4 * g + 2], hi[4 * g + 3]}, w[g]);
+        for (int g = 0; g < 4; ++g) {
+          uint32_t lo[4], hi[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const unsigned long long y = i8::data_word(part ? x[4 * g + i].y : x[4 * g + i].x, sc);
+            lo[i] = (uint32_t)y;
+            hi[i] = (uint32_t)(y >> 32);
+          }
+          i8::digit_words_data(lo, hi, w[g]);
+        }
         const uint32_t off = canon(2 * cl + part, q);
 #pragma unroll
         for (int s = 0; s < kDigitsData; ++s)
