@@ -4,7 +4,7 @@ It serves callers that must not allocate device memory while they run.  Those
 are hosts whose GPU memory belongs to another pool allocator, time loops that
 cannot take the synchronisation cudaMalloc may cause, and hosts that forbid
 allocation after start-up.  Its output must match the ordinary device entry
-point, sht_wa_xya_dev, on two calls in a row.  Two calls matter because the
+point, sht_wa_xya_dev, and the oracle's analysis on two calls in a row.  Two calls matter because the
 fixed scratch array keeps the first call's data.  A batch larger than the
 fixed scratch must be refused cleanly.
 
@@ -17,6 +17,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import oracle as O
 from conftest import pkg, relerr, workloads
 
 pytestmark = pytest.mark.gpu
@@ -63,6 +64,8 @@ def test_noalloc_matches_device_entry_point_twice():
             assert np.isfinite(o).all(), f"call {call}: non-finite output"
             assert relerr(o, r) < TOL, f"call {call}: {relerr(o, r)}"
             assert relerr(o, w.cpu().numpy()) < TOL, f"call {call}: round trip"
+            # and against the oracle's analysis of the same grid
+            assert relerr(o, O.OraclePlan(I, J, N, 6.371e6).wa_xya(grid.cpu().numpy())) < TOL, f"call {call}: oracle"
     finally:
         sht.final()
 
