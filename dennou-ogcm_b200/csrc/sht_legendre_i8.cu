@@ -71,6 +71,10 @@ template <bool INV>
 struct Roles {
   static constexpr int kConvW = INV ? 4 : 8, kEpiW = INV ? 8 : 4;
   static constexpr int kConv0 = 2, kEpi0 = kConv0 + kConvW;
+  // values per thread in flight in the column-exponent pass over a sub-item's
+  // other K chunks: 16 in the synthesis (strided coefficient rows), 4 in the
+  // analysis (contiguous Fourier runs; 16 measured slower at T341)
+  static constexpr int kPreBatch = INV ? 16 : 4;
   static constexpr int kThreads = 32 * (kEpi0 + kEpiW);
 };
 constexpr int kThreads = 448;
@@ -407,23 +411,14 @@ __device__ void role_mma(const I8Args &a, const Ctl &c, uint32_t As, uint32_t Ps
   tc::mma_commit(c.bar + B_DONE);
 }
 
-// K value k of this thread's complex column (zero past the end).
-template <bool INV>
-__device__ __forceinline__ double2 load1(const I8Args &a, const Unit &u, int col, bool cv, int k)
-{
-  if (!cv || k >= u.K) return make_double2(0.0, 0.0);
-  return INV ? a.Sc[((long long)u.rowoff + u.p + 2 * k) * a.ncol + col]
-             : a.F[((long long)u.m * a.ncol + col) * a.J + u.p * a.JH + k];
-}
-
-// Load 16 consecutive K values (k0 + i) of this thread's complex column.
-template <bool INV>
-__device__ __forceinline__ void load16(const I8Args &a, const Unit &u, int col, bool cv, int k0, double2 (&x)[16])
+// Load NV consecutive K values (k0 + i) of this thread's complex column.
+template <bool INV, int NV>
+__device__ __forceinline__ void loadn(const I8Args &a, const Unit &u, int col, bool cv, int k0, double2 (&x)[NV])
 {
   if (!INV) {
     const double2 *src = a.F + ((long long)u.m * a.ncol + (cv ? col : 0)) * a.J + u.p * a.JH;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) x[i] = (cv && k0 + i < u.K) ? src[k0 + i] : make_double2(0.0, 0.0);
+    for (int i = 0; i < NV; ++i) x[i] = (cv && k0 + i < u.K) ? src[k0 + i] : make_double2(0.0, 0.0);
   } else {
     // one row pointer advanced by two internal rows (one parity) per value:
     // no per-value 64-bit index products held for the whole batch of loads
@@ -431,10 +426,27 @@ __device__ __forceinline__ void load16(const I8Args &a, const Unit &u, int col, 
     const double2 *src = a.Sc + ((long long)u.rowoff + u.p + 2 * k0) * a.ncol + (cv ? col : 0);
     const int nv = cv ? u.K - k0 : 0;
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
+    for (int i = 0; i < NV; ++i) {
       x[i] = i < nv ? *src : make_double2(0.0, 0.0);
       src += step;
     }
+  }
+}
+template <bool INV>
+__device__ __forceinline__ void load16(const I8Args &a, const Unit &u, int col, bool cv, int k0, double2 (&x)[16])
+{
+  loadn<INV, 16>(a, u, col, cv, k0, x);
+}
+
+// r, im <- the largest high word (sign cleared) of the real and imaginary
+// parts of NV values and r, im
+template <int NV>
+__device__ __forceinline__ void hmaxn(const double2 (&y)[NV], int &r, int &im)
+{
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    r = max(r, __double2hiint(y[i].x) & 0x7FFFFFFF);
+    im = max(im, __double2hiint(y[i].y) & 0x7FFFFFFF);
   }
 }
 
@@ -467,43 +479,41 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
       // the exponent of a column's largest magnitude is that of the largest
       // high word (sign cleared): integer maxima, no FP64 chain
       int mr = 0, mi = 0;
-      if (first && u.nch > 1) {
-        // column exponents over every K chunk of the sub-item, before this
-        // chunk's values take their registers
-        for (int kk = 16 * q; kk < u.K; kk += kKC) {
-#pragma unroll 1
-          for (int i0 = 0; i0 < 16; i0 += 4) {
-            double2 y[4];
+      // the largest high word (sign cleared) of 16 values
+      auto hmax = [](const double2 (&y)[16], int &r, int &im) {
+        int hr[8], hi[8];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) y[i] = load1<INV>(a, u, col, cv, kk + i0 + i);
-#pragma unroll
-            for (int i = 0; i < 4; ++i) {
-              mr = max(mr, __double2hiint(y[i].x) & 0x7FFFFFFF);
-              mi = max(mi, __double2hiint(y[i].y) & 0x7FFFFFFF);
-            }
-          }
+        for (int i = 0; i < 8; ++i) {
+          hr[i] = max(__double2hiint(y[i].x) & 0x7FFFFFFF, __double2hiint(y[i + 8].x) & 0x7FFFFFFF);
+          hi[i] = max(__double2hiint(y[i].y) & 0x7FFFFFFF, __double2hiint(y[i + 8].y) & 0x7FFFFFFF);
         }
+#pragma unroll
+        for (int w = 4; w >= 1; w >>= 1)
+#pragma unroll
+          for (int i = 0; i < w; ++i) {
+            hr[i] = max(hr[i], hr[i + w]);
+            hi[i] = max(hi[i], hi[i + w]);
+          }
+        r = max(r, hr[0]);
+        im = max(im, hi[0]);
+      };
+      if (first) {
+        // column exponents over the sub-item's other K chunks (the first
+        // unit converts chunk 0), kPreBatch values of this thread in flight
+        // at a time, before this chunk's values take their registers
+        constexpr int PB = Roles<INV>::kPreBatch;
+        for (int kc = 1; kc < u.nch; ++kc)
+#pragma unroll 1
+          for (int i0 = 0; i0 < 16; i0 += PB) {
+            double2 y[PB];
+            loadn<INV, PB>(a, u, col, cv, kc * kKC + 16 * q + i0, y);
+            hmaxn<PB>(y, mr, mi);
+          }
       }
       double2 x[16];
       load16<INV>(a, u, col, cv, k0, x);
       if (first) {
-        if (u.nch == 1) {
-          int hr[8], hi[8];
-#pragma unroll
-          for (int i = 0; i < 8; ++i) {
-            hr[i] = max(__double2hiint(x[i].x) & 0x7FFFFFFF, __double2hiint(x[i + 8].x) & 0x7FFFFFFF);
-            hi[i] = max(__double2hiint(x[i].y) & 0x7FFFFFFF, __double2hiint(x[i + 8].y) & 0x7FFFFFFF);
-          }
-#pragma unroll
-          for (int w = 4; w >= 1; w >>= 1)
-#pragma unroll
-            for (int i = 0; i < w; ++i) {
-              hr[i] = max(hr[i], hr[i + w]);
-              hi[i] = max(hi[i], hi[i + w]);
-            }
-          mr = hr[0];
-          mi = hi[0];
-        }
+        hmax(x, mr, mi);
         mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, 8));
         mr = max(mr, __shfl_xor_sync(0xffffffffu, mr, 16));
         mi = max(mi, __shfl_xor_sync(0xffffffffu, mi, 8));
