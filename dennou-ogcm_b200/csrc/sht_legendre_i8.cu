@@ -86,7 +86,7 @@ static_assert(kLevels * kSeg <= kSetCols && 2 * kSetCols <= 512, "TMEM columns")
 // barrier indices
 enum : int {
   B_PFULL = 0, B_PEMPTY = 2, B_DFULL = 4, B_DEMPTY = 6, B_AFULL = 8, B_AEMPTY = 10,
-  B_EFULL = 12, B_EEMPTY = 16, B_DONE = 20, B_COUNT = 21
+  B_EFULL = 12, B_EEMPTY = 16, B_DONE = 20, B_CFULL = 21, B_SREADY = 23, B_COUNT = 25
 };
 
 __host__ __device__ inline int rows_of_parity(int N, int m, int p)
@@ -111,6 +111,8 @@ struct I8Tables {
   long long *toff[2] = {nullptr, nullptr};   // byte offset per (m, p)
   double *tfac[2] = {nullptr, nullptr};      // row scale factors 2^(e_row - kShift)
   int *teoff[2] = {nullptr, nullptr};        // first row exponent per (m, p)
+  uint8_t *scr[2] = {nullptr, nullptr};      // digit cache: per CTA, two slots of the chunks of one sub-item
+  long long scr_cta[2] = {0, 0};             // its bytes per CTA
   int *d_err = nullptr;                      // device error word
 };
 
@@ -170,6 +172,8 @@ struct I8Args {
   int N, J, JH, ncol, npairs;
   int ntiles, nsub, per_cta;
   int *err;
+  uint8_t *scr;        // digit cache (null when no sub-item has more than two segments)
+  long long scr_cta;   // bytes of it per CTA: two slots of nchmax data stages
 };
 
 // Shared-memory copies of the small lookup tables (band pairs, internal row
@@ -196,6 +200,7 @@ struct Unit {
   int col0;
   int sub_count;          // sub-items this CTA began before this one
   int seg_base;           // segments this CTA began before this sub-item
+  int csub;               // sub-items with more than two segments this CTA began before this one
   int rowoff, teoff;      // internal row of degree m, first row factor of (m, p)
   long long toff;         // table bytes of (m, p)
 };
@@ -230,6 +235,7 @@ __device__ __forceinline__ bool first_unit(const I8Args &a, const Lut &t, int g0
     if (setup_sub<INV>(a, t, g, u)) {
       u.sub_count = 0;
       u.seg_base = 0;
+      u.csub = 0;
       return true;
     }
   return false;
@@ -241,14 +247,25 @@ __device__ __forceinline__ bool next_unit(const I8Args &a, const Lut &t, int g1,
   if (++u.ch < u.nch) return true;
   u.ch = 0;
   if ((u.seg += 2) < u.nseg) return true;
-  const int sc = u.sub_count + 1, sb = u.seg_base + u.nseg;
+  const int sc = u.sub_count + 1, sb = u.seg_base + u.nseg, cs = u.csub + (u.nseg > 2 ? 1 : 0);
   for (int g = u.g + 1; g < g1; ++g)
     if (setup_sub<INV>(a, t, g, u)) {
       u.sub_count = sc;
       u.seg_base = sb;
+      u.csub = cs;
       return true;
     }
   return false;
+}
+
+// Digit cache: a sub-item with more than two output segments is converted by
+// the converters once, in its first segment group, which also writes the
+// digit stages to the CTA's cache slot; its later groups take the stages from
+// there by bulk copy.
+__device__ __forceinline__ bool unit_cached(const Unit &u) { return u.nseg > 2 && u.seg >= 2; }
+__device__ __forceinline__ uint8_t *cache_stage(const I8Args &a, const Unit &u)
+{
+  return a.scr + blockIdx.x * a.scr_cta + (u.csub & 1) * (a.scr_cta / 2) + (long long)u.ch * kStageA;
 }
 
 struct Ctl {
@@ -325,10 +342,12 @@ __device__ __forceinline__ void epilogue_rows(const I8Args &a, const Unit &u, in
 
 // ---------------------------------------------------------------- roles
 
-template <bool INV>
-__device__ void role_producer(const I8Args &a, const Ctl &c, unsigned char *Ps, const Lut &t, Unit u, bool have, int g1)
+template <bool INV, bool CACHE>
+__device__ void role_producer(const I8Args &a, const Ctl &c, unsigned char *Ps, unsigned char *As, const Lut &t, Unit u,
+                              bool have, int g1)
 {
-  int k = 0;
+  int k = 0, nc[2] = {0, 0};
+  int cpend[2] = {-1, -1};  // phase parity of the last cache copy into each data stage
   for (; have; have = next_unit<INV>(a, t, g1, u), ++k) {
     const int st = k & 1;
     if (k >= 2 && !wait_ph(c, B_PEMPTY + st, ((k >> 1) - 1) & 1)) break;
@@ -345,19 +364,35 @@ __device__ void role_producer(const I8Args &a, const Ctl &c, unsigned char *Ps, 
       tc::bulk_g2s(Ps + st * kStageP + off, src + off, b, c.bar + B_PFULL + st);
       off += b;
     }
+    if (CACHE && unit_cached(u)) {
+      // the data digits of a later segment group: the converters wrote them to
+      // the cache slot in the sub-item's first group; the stage is free once
+      // the MMAs of unit k - 2 are done
+      if (u.seg == 2 && u.ch == 0 && !wait_ph(c, B_SREADY + (u.csub & 1), (u.csub >> 1) & 1)) break;
+      if (k >= 2 && !wait_ph(c, B_DEMPTY + st, ((k >> 1) - 1) & 1)) break;
+      tc::mbar_arrive_expect_tx(c.bar + B_CFULL + st, kStageA);
+      tc::bulk_g2s(As + st * kStageA, cache_stage(a, u), kStageA, c.bar + B_CFULL + st);
+      cpend[st] = nc[st] & 1;
+      ++nc[st];
+    }
   }
   // copies issued but never consumed (after an abort) must land before the CTA exits
   for (int j = (k >= 2 ? k - 2 : 0); j < k; ++j) wait_ph(Ctl{c.bar, c.abort_flag, c.err}, B_PFULL + (j & 1), (j >> 1) & 1);
+  for (int st = 0; st < 2; ++st)
+    if (cpend[st] >= 0) wait_ph(c, B_CFULL + st, (uint32_t)cpend[st]);
 }
 
-template <bool INV>
+template <bool INV, bool CACHE>
 __device__ void role_mma(const I8Args &a, const Ctl &c, uint32_t As, uint32_t Ps, uint32_t tbase, const Lut &t, Unit u, bool have, int g1)
 {
-  int k = 0;
+  int k = 0, nd[2] = {0, 0}, nc[2] = {0, 0};
   for (; have; have = next_unit<INV>(a, t, g1, u), ++k) {
     const int st = k & 1;
     if (!wait_ph(c, B_PFULL + st, (k >> 1) & 1)) break;
-    if (!wait_ph(c, B_DFULL + st, (k >> 1) & 1)) break;
+    // the data stage comes from the converters or, for a cached unit, from
+    // the producer's copy of the digit cache
+    if ((CACHE && unit_cached(u)) ? !wait_ph(c, B_CFULL + st, nc[st]++ & 1) : !wait_ph(c, B_DFULL + st, nd[st]++ & 1))
+      break;
     tc::fence_after();
     const int s0 = u.seg, s1 = min(u.seg + 2, u.nseg);
     const int kvalid = min(kKC, u.K - u.ch * kKC);
@@ -450,7 +485,7 @@ __device__ __forceinline__ void hmaxn(const double2 (&y)[NV], int &r, int &im)
   }
 }
 
-template <bool INV>
+template <bool INV, bool CACHE>
 __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, int *exps, const Lut &t, Unit u, bool have, int g1)
 {
   using R = Roles<INV>;
@@ -465,7 +500,16 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
   int k = 0;
   for (; have; have = next_unit<INV>(a, t, g1, u), ++k) {
     const int st = k & 1;
+    if (CACHE && unit_cached(u)) {
+      // the producer copies these digits from the cache; the converters still
+      // step through the stage's phases one at a time (a parity wait only
+      // tells the last two phases apart), so they wait for unit k - 2 here
+      if (k >= 2 && !warp_wait(c, B_DEMPTY + st, ((k >> 1) - 1) & 1)) break;
+      continue;
+    }
     const int k0 = u.ch * kKC + 16 * q;
+    // a sub-item with more than two segments keeps its digits for its later groups
+    uint8_t *const cache = (CACHE && u.nseg > 2) ? cache_stage(a, u) : nullptr;
     const bool first = u.seg == 0 && u.ch == 0;
     const int slot = u.sub_count & (kSlots - 1);
     if (first && u.sub_count >= kSlots && !warp_wait(c, B_EEMPTY + slot, (u.sub_count / kSlots - 1) & 1)) break;
@@ -560,8 +604,11 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
         }
         const uint32_t off = canon(2 * cl + part, q);
 #pragma unroll
-        for (int s = 0; s < kDigitsData; ++s)
-          *reinterpret_cast<uint4 *>(stage + s * kTileA + off) = make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
+        for (int s = 0; s < kDigitsData; ++s) {
+          const uint4 d4 = make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
+          *reinterpret_cast<uint4 *>(stage + s * kTileA + off) = d4;
+          if (cache) *reinterpret_cast<uint4 *>(cache + s * kTileA + off) = d4;
+        }
       }
     }
     if (!ok) break;
@@ -570,8 +617,13 @@ __device__ void role_convert(const I8Args &a, const Ctl &c, unsigned char *As, i
       if (lane == 0) tc::mbar_arrive(c.bar + B_EFULL + slot);
     }
     tc::fence_proxy_async();
+    if (cache) tc::fence_proxy_async_global();
     __syncwarp();
-    if (lane == 0) tc::mbar_arrive(c.bar + B_DFULL + st);
+    if (lane == 0) {
+      tc::mbar_arrive(c.bar + B_DFULL + st);
+      // the sub-item's first group is written to the cache: its later groups may be copied
+      if (cache && u.ch == u.nch - 1) tc::mbar_arrive(c.bar + B_SREADY + (u.csub & 1));
+    }
   }
 }
 
@@ -633,7 +685,7 @@ __device__ void role_epilogue(const I8Args &a, const Ctl &c, const int *exps, ui
   }
 }
 
-template <bool INV>
+template <bool INV, bool CACHE>
 __global__ void __launch_bounds__(kThreads, 1) k_leg_i8(I8Args a)
 {
   extern __shared__ __align__(1024) unsigned char smem[];
@@ -677,6 +729,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_i8(I8Args a)
       tc::mbar_init(bar + B_EFULL + i, Roles<INV>::kConvW);
       tc::mbar_init(bar + B_EEMPTY + i, Roles<INV>::kEpiW);
     }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(bar + B_CFULL + i, 1);
+      tc::mbar_init(bar + B_SREADY + i, Roles<INV>::kConvW);
+    }
     tc::mbar_init(bar + B_DONE, 1);
     abort_flag = 0;
     tc::mbar_fence_init();
@@ -690,11 +746,11 @@ __global__ void __launch_bounds__(kThreads, 1) k_leg_i8(I8Args a)
   Unit u;
   const bool have = first_unit<INV>(a, t, g0, g1, u);
   if (warp == 0) {
-    if (lane == 0) role_producer<INV>(a, c, Ps, t, u, have, g1);
+    if (lane == 0) role_producer<INV, CACHE>(a, c, Ps, As, t, u, have, g1);
   } else if (warp == 1) {
-    if (lane == 0) role_mma<INV>(a, c, tc::smem_addr(As), tc::smem_addr(Ps), tbase, t, u, have, g1);
+    if (lane == 0) role_mma<INV, CACHE>(a, c, tc::smem_addr(As), tc::smem_addr(Ps), tbase, t, u, have, g1);
   } else if (warp < Roles<INV>::kEpi0) {
-    role_convert<INV>(a, c, As, exps, t, u, have, g1);
+    role_convert<INV, CACHE>(a, c, As, exps, t, u, have, g1);
   } else {
     role_epilogue<INV>(a, c, exps, tbase, t, u, have, g1);
   }
@@ -740,7 +796,7 @@ int build_i8_tables(sht_plan *p)
   cudaError_t e = cudaSuccess;
   auto fail = [&](cudaError_t err, const char *what) {
     for (int d = 0; d < 2; ++d) {
-      cudaFree(t->tab[d]); cudaFree(t->toff[d]); cudaFree(t->tfac[d]); cudaFree(t->teoff[d]);
+      cudaFree(t->tab[d]); cudaFree(t->toff[d]); cudaFree(t->tfac[d]); cudaFree(t->teoff[d]); cudaFree(t->scr[d]);
     }
     cudaFree(t->d_err);
     delete t;
@@ -756,6 +812,15 @@ int build_i8_tables(sht_plan *p)
         (e = cudaMemcpyAsync(t->toff[d], toff[d].data(), sizeof(long long) * nmp, cudaMemcpyHostToDevice, s)) != cudaSuccess ||
         (e = cudaMemcpyAsync(t->teoff[d], teoff[d].data(), sizeof(int) * nmp, cudaMemcpyHostToDevice, s)) != cudaSuccess)
       return fail(e, "split table upload");
+  }
+  // digit cache for sub-items with more than two 32-row output segments:
+  // analysis rows are the degrees of one parity, synthesis rows the latitudes
+  for (int d = 0; d < 2; ++d) {
+    const int nrow = d ? JH : (N + 3) / 2, K = d ? (N + 3) / 2 : JH;
+    if (nrow <= 2 * kSeg) continue;
+    t->scr_cta[d] = 2LL * ((K + kKC - 1) / kKC) * kStageA;
+    const size_t bytes = (size_t)t->scr_cta[d] * (p->num_sms > 0 ? p->num_sms : 1);
+    if ((e = cudaMalloc(&t->scr[d], bytes)) != cudaSuccess) return fail(e, "split digit cache");
   }
   if ((e = cudaMalloc(&t->d_err, sizeof(int))) != cudaSuccess) return fail(e, "split table");
   if ((e = cudaMemsetAsync(t->d_err, 0, sizeof(int), s)) != cudaSuccess) return fail(e, "split table upload");
@@ -789,13 +854,17 @@ int launch_i8(sht_plan *p, bool inverse, const double2 *in, int ncol, double2 *o
   if (inverse) { a.Sc = in; a.Fo = out; } else { a.F = in; a.S = out; }
   a.rowoff = p->d_rowoff; a.pairs = p->d_pairs;
   a.tab = t->tab[d]; a.toff = t->toff[d]; a.tfac = t->tfac[d]; a.teoff = t->teoff[d];
+  a.scr = t->scr[d]; a.scr_cta = t->scr_cta[d];
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol; a.err = t->d_err; a.npairs = p->n_pairs;
   a.ntiles = (ncol + kM / 2 - 1) / (kM / 2);
   a.nsub = 4 * p->n_pairs * a.ntiles;
   const int slots = p->num_sms > 0 ? p->num_sms : 1;
   a.per_cta = (a.nsub + slots - 1) / slots;
   const int grid = (a.nsub + a.per_cta - 1) / a.per_cta;
-  auto kern = inverse ? k_leg_i8<true> : k_leg_i8<false>;
+  // the digit-cache instance where some sub-item has more than two output
+  // segments (T170 and up), the plain one elsewhere
+  auto kern = inverse ? (a.scr ? k_leg_i8<true, true> : k_leg_i8<true, false>)
+                      : (a.scr ? k_leg_i8<false, true> : k_leg_i8<false, false>);
   const size_t smem = kSmemFixed + lut_bytes(p->N, p->n_pairs);
   if (smem > 227 * 1024) {
     set_error("split precision: the truncation's lookup tables do not fit beside the stages");
@@ -880,7 +949,7 @@ void free_split_tables(sht_plan *p)
   I8Tables *t = tables(p);
   if (!t) return;
   for (int d = 0; d < 2; ++d) {
-    cudaFree(t->tab[d]); cudaFree(t->toff[d]); cudaFree(t->tfac[d]); cudaFree(t->teoff[d]);
+    cudaFree(t->tab[d]); cudaFree(t->toff[d]); cudaFree(t->tfac[d]); cudaFree(t->teoff[d]); cudaFree(t->scr[d]);
   }
   cudaFree(t->d_err);
   delete t;
