@@ -750,7 +750,7 @@ int run_dft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
   int occ = 0;
   cudaError_t e = kernel_setup((const void *)kern, smem, kDftThreads, &occ);
   if (e != cudaSuccess) return cuda_fail(e, "dft smem attribute");
-  const long long g = (long long)(occ < 1 ? 1 : occ) * (p->num_sms > 0 ? p->num_sms : 1);
+  const long long g = (long long)(occ < 1 ? 1 : occ) * grid_sms(p);
   kern<<<(int)(ntiles < g ? ntiles : g), kDftThreads, smem, s>>>(a);
   count_launch();
   e = cudaGetLastError();
@@ -774,7 +774,7 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
   auto go = [&](auto kern, auto... extra) {
     int occ = 0;
     if ((e = kernel_setup((const void *)kern, smem, kFftThreads, &occ)) != cudaSuccess) return;
-    const long long g = (long long)(occ < 1 ? 1 : occ) * (p->num_sms > 0 ? p->num_sms : 1);
+    const long long g = (long long)(occ < 1 ? 1 : occ) * grid_sms(p);
     kern<<<(int)(ntiles < g ? ntiles : g), kFftThreads, smem, s>>>(a, extra...);
   };
   if (inverse) go(k_fft_inv<A, B, kFftThreads>, bufe);

@@ -109,6 +109,7 @@ struct sht_plan_s {
   int2 *d_pairs = nullptr;       // band pairs (m, N-m), (N/2, -1) for even N
   int n_pairs = 0;
   int num_sms = 0;
+  int sm_cap = 0;       // at most this many SMs' worth of persistent blocks (0: all); set by a batch that runs plans side by side
 
   // host copies
   std::vector<double> h_mu, h_wgt;
@@ -179,6 +180,12 @@ int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *
 int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 
 // --- persistent paired-band FP64 contraction (sht_legendre_v2.cu)
+// SMs a plan's persistent kernels size their grids for
+inline int grid_sms(const sht_plan *p)
+{
+  const int n = p->num_sms > 0 ? p->num_sms : 1;
+  return (p->sm_cap > 0 && p->sm_cap < n) ? p->sm_cap : n;
+}
 bool leg_pair_supported(const sht_plan *p);
 int launch_leg_fwd_pair(const sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_pair(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);

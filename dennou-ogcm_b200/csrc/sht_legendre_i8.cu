@@ -858,7 +858,7 @@ int launch_i8(sht_plan *p, bool inverse, const double2 *in, int ncol, double2 *o
   a.N = p->N; a.J = p->J; a.JH = p->JH; a.ncol = ncol; a.err = t->d_err; a.npairs = p->n_pairs;
   a.ntiles = (ncol + kM / 2 - 1) / (kM / 2);
   a.nsub = 4 * p->n_pairs * a.ntiles;
-  const int slots = p->num_sms > 0 ? p->num_sms : 1;
+  const int slots = grid_sms(p);  // never above the SM count the digit cache is sized for
   a.per_cta = (a.nsub + slots - 1) / slots;
   const int grid = (a.nsub + a.per_cta - 1) / a.per_cta;
   // the digit-cache instance where some sub-item has more than two output

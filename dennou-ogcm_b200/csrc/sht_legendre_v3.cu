@@ -401,7 +401,7 @@ int run(K kern, size_t smem, const sht_plan *p, V3Args &a, cudaStream_t s, const
   int per_sm = 0;
   cudaError_t e = kernel_setup((const void *)kern, smem, kT, &per_sm);
   if (e != cudaSuccess || per_sm < 1) return cuda_fail(e == cudaSuccess ? cudaErrorInvalidConfiguration : e, name);
-  const int slots = p->num_sms * per_sm;
+  const int slots = grid_sms(p) * per_sm;
   a.per_cta = (a.nitems + slots - 1) / slots;
   const int grid = (a.nitems + a.per_cta - 1) / a.per_cta;
   kern<<<grid, kT, smem, s>>>(a);

@@ -37,6 +37,7 @@ struct Group {
   double **d_wcol = nullptr;        // ncol spectral column pointers (device)
   double2 *F = nullptr, *S = nullptr;
   int precision = SHT_PREC_FP64, leg_kernel = 0, leg_tile = 0;
+  int sm_cap = 0;               // SMs its persistent kernels size their grids for (0: all)
   float tuned_ms = 0.f;
   cudaEvent_t join = nullptr;
 };
@@ -81,14 +82,14 @@ bool live(const sht_multi *m) { return m && m->magic == kMultiMagic; }
 // order) and points each plan at its own stream with the group's Legendre
 // configuration; everything is restored on release.
 struct PlanLease {
-  struct Saved { sht_plan *p; cudaStream_t stream; int precision, leg_kernel, leg_tile; bool timing; };
+  struct Saved { sht_plan *p; cudaStream_t stream; int precision, leg_kernel, leg_tile, sm_cap; bool timing; };
   std::vector<Saved> saved;
   explicit PlanLease(sht_multi *m)
   {
     for (Group &g : m->groups) {
       g.plan->mtx.lock();
       saved.push_back({g.plan, g.plan->stream, g.plan->precision, g.plan->leg_kernel, g.plan->leg_tile,
-                       g.plan->timing.on});
+                       g.plan->sm_cap, g.plan->timing.on});
       g.plan->stream = g.plan->own_stream;
       g.plan->timing.on = false;
       apply(g);
@@ -99,6 +100,7 @@ struct PlanLease {
     g.plan->precision = g.precision;
     g.plan->leg_kernel = g.leg_kernel;
     g.plan->leg_tile = g.leg_tile;
+    g.plan->sm_cap = g.sm_cap;
   }
   ~PlanLease()
   {
@@ -107,6 +109,7 @@ struct PlanLease {
       it->p->precision = it->precision;
       it->p->leg_kernel = it->leg_kernel;
       it->p->leg_tile = it->leg_tile;
+      it->p->sm_cap = it->sm_cap;
       it->p->timing.on = it->timing;
       it->p->mtx.unlock();
     }
@@ -215,6 +218,61 @@ int tune_group(Group &g, bool allow_split)
   return SHT_OK;
 }
 
+// Mean time of `reps` eager round-trip steps of the whole batch.
+int time_step(sht_multi *m, int reps, float *ms)
+{
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaError_t e;
+  int rc = SHT_OK;
+  if ((e = cudaEventCreate(&a)) != cudaSuccess || (e = cudaEventCreate(&b)) != cudaSuccess) {
+    rc = cuda_fail(e, "tuner events");
+  } else {
+    rc = enqueue_step(m, SHT_MULTI_ROUND_TRIP, m->stream);  // warm-up
+    if (!rc) cudaEventRecord(a, m->stream);
+    for (int r = 0; r < reps && !rc; ++r) rc = enqueue_step(m, SHT_MULTI_ROUND_TRIP, m->stream);
+    if (!rc) {
+      cudaEventRecord(b, m->stream);
+      if ((e = cudaEventSynchronize(b)) != cudaSuccess) rc = cuda_fail(e, "tuner timing");
+    }
+    if (!rc) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, a, b);
+      *ms = t / reps;
+    }
+  }
+  if (a) cudaEventDestroy(a);
+  if (b) cudaEventDestroy(b);
+  return rc ? rc : check_device_errors(m);
+}
+
+// The groups run on their own streams, but each persistent kernel sizes its
+// grid for the whole GPU, so a kernel of one group waits for the SMs another
+// holds.  Alternatively every group's persistent kernels are sized for a
+// share of the SMs in proportion to its tuned time, so that the groups run
+// side by side; the tuner keeps whichever step measures faster.
+int tune_partition(sht_multi *m)
+{
+  float whole = 0.f, split = 0.f, sum = 0.f;
+  int rc = time_step(m, 3, &whole);
+  if (rc) return rc;
+  for (const Group &g : m->groups) sum += g.tuned_ms;
+  if (!(sum > 0.f)) return SHT_OK;
+  const int nsm = m->groups.front().plan->num_sms;
+  for (Group &g : m->groups) {
+    const int share = (int)(nsm * (g.tuned_ms / sum) + 0.5f);
+    g.sm_cap = share < 4 ? 4 : share;
+    PlanLease::apply(g);
+  }
+  if ((rc = time_step(m, 3, &split))) return rc;
+  if (!(split < whole)) {
+    for (Group &g : m->groups) {
+      g.sm_cap = 0;
+      PlanLease::apply(g);
+    }
+  }
+  return SHT_OK;
+}
+
 void free_groups(sht_multi *m)
 {
   for (auto &x : m->exec)
@@ -276,6 +334,7 @@ int build(sht_multi *m, int flags)
   if ((rc = enqueue_step(m, SHT_MULTI_ROUND_TRIP, m->stream))) return rc;
   if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "multi warm-up");
   if ((rc = check_device_errors(m))) return rc;
+  if ((flags & SHT_MULTI_AUTOTUNE) && m->groups.size() > 1 && (rc = tune_partition(m))) return rc;
 
   // Capture each step kind: the graph is kept for replay unless the batch
   // runs stage by stage, and the capture counts the kernels of one step.
@@ -411,6 +470,16 @@ int sht_multi_group_info(const sht_multi *m, int group, int *ncol, int *precisio
   if (precision) *precision = g.precision;
   if (legendre_kernel) *legendre_kernel = g.leg_kernel;
   if (tuned_ms) *tuned_ms = g.tuned_ms;
+  return SHT_OK;
+}
+
+int sht_multi_group_sms(const sht_multi *m, int group, int *sms)
+{
+  if (!live(m) || !sms || group < 0 || group >= (int)m->groups.size()) {
+    set_error("multi: bad group");
+    return SHT_ERR_INVALID_ARG;
+  }
+  *sms = m->groups[group].sm_cap;
   return SHT_OK;
 }
 

@@ -124,6 +124,7 @@ def load_library(path: str | None = None):
     lib.sht_multi_group_info.argtypes = [_VP, ctypes.c_int] + [ctypes.POINTER(ctypes.c_int)] * 3 + \
         [ctypes.POINTER(ctypes.c_float)]
     lib.sht_multi_group_tile.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+    lib.sht_multi_group_sms.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_kernels.argtypes = [_VP, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
     lib.sht_multi_destroy.argtypes = [_VP]
     _lib = lib
@@ -578,7 +579,7 @@ class MultiTransform:
         _check(self._lib.sht_multi_set_stream(self._h, stream.cuda_stream), "sht_multi_set_stream")
 
     def groups(self):
-        """Per plan group: dict(ncol, precision, legendre_kernel, legendre_tile, tuned_ms)."""
+        """Per plan group: dict(ncol, precision, legendre_kernel, legendre_tile, sms, tuned_ms)."""
         n = ctypes.c_int()
         _check(self._lib.sht_multi_groups(self._h, ctypes.byref(n)), "sht_multi_groups")
         out = []
@@ -586,10 +587,11 @@ class MultiTransform:
             nc, pr, lk, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_float()
             _check(self._lib.sht_multi_group_info(self._h, g, ctypes.byref(nc), ctypes.byref(pr), ctypes.byref(lk),
                                                   ctypes.byref(ms)), "sht_multi_group_info")
-            tile = ctypes.c_int()
+            tile, sms = ctypes.c_int(), ctypes.c_int()
             _check(self._lib.sht_multi_group_tile(self._h, g, ctypes.byref(tile)), "sht_multi_group_tile")
+            _check(self._lib.sht_multi_group_sms(self._h, g, ctypes.byref(sms)), "sht_multi_group_sms")
             out.append(dict(ncol=nc.value, precision=pr.value, legendre_kernel=lk.value, legendre_tile=tile.value,
-                            tuned_ms=ms.value))
+                            sms=sms.value, tuned_ms=ms.value))
         return out
 
     def kernels(self, what: int = SHT_MULTI_ROUND_TRIP) -> int:

@@ -416,6 +416,10 @@ SHT_API int sht_multi_group_info(const sht_multi *multi, int group, int *ncol, i
                                  int *legendre_kernel, float *tuned_ms);
 /* The SHT_OPT_LEGENDRE_TILE value the group runs with (the tuner's choice). */
 SHT_API int sht_multi_group_tile(const sht_multi *multi, int group, int *legendre_tile);
+/* SMs the group's persistent kernels size their grids for, so that the
+ * groups run side by side (0: the whole GPU).  With autotuning the build
+ * times the batch both ways and keeps the faster. */
+SHT_API int sht_multi_group_sms(const sht_multi *multi, int group, int *sms);
 /* Kernel launches one sht_multi_run(what) replays. */
 SHT_API int sht_multi_kernels(const sht_multi *multi, int what, int *nkernels);
 SHT_API int sht_multi_destroy(sht_multi *multi);
