@@ -248,21 +248,28 @@ int time_step(sht_multi *m, int reps, float *ms)
 // The groups run on their own streams, but each persistent kernel sizes its
 // grid for the whole GPU, so a kernel of one group waits for the SMs another
 // holds.  Alternatively every group's persistent kernels are sized for a
-// share of the SMs in proportion to its tuned time, so that the groups run
-// side by side; the tuner keeps whichever step measures faster.
-int tune_partition(sht_multi *m)
+// share of the SMs in proportion to its tuned time (its columns when not
+// tuned), so that the groups run side by side.
+void share_sms(sht_multi *m)
 {
-  float whole = 0.f, split = 0.f, sum = 0.f;
-  int rc = time_step(m, 3, &whole);
-  if (rc) return rc;
-  for (const Group &g : m->groups) sum += g.tuned_ms;
-  if (!(sum > 0.f)) return SHT_OK;
+  float sum = 0.f;
+  for (const Group &g : m->groups) sum += g.tuned_ms > 0.f ? g.tuned_ms : (float)g.ncol;
   const int nsm = m->groups.front().plan->num_sms;
   for (Group &g : m->groups) {
-    const int share = (int)(nsm * (g.tuned_ms / sum) + 0.5f);
+    const float w = g.tuned_ms > 0.f ? g.tuned_ms : (float)g.ncol;
+    const int share = (int)(nsm * (w / sum) + 0.5f);
     g.sm_cap = share < 4 ? 4 : share;
     PlanLease::apply(g);
   }
+}
+
+// the tuner keeps whichever of whole-GPU grids and shared SMs measures faster
+int tune_partition(sht_multi *m)
+{
+  float whole = 0.f, split = 0.f;
+  int rc = time_step(m, 3, &whole);
+  if (rc) return rc;
+  share_sms(m);
   if ((rc = time_step(m, 3, &split))) return rc;
   if (!(split < whole)) {
     for (Group &g : m->groups) {
@@ -334,7 +341,14 @@ int build(sht_multi *m, int flags)
   if ((rc = enqueue_step(m, SHT_MULTI_ROUND_TRIP, m->stream))) return rc;
   if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "multi warm-up");
   if ((rc = check_device_errors(m))) return rc;
-  if ((flags & SHT_MULTI_AUTOTUNE) && m->groups.size() > 1 && (rc = tune_partition(m))) return rc;
+  if (flags & SHT_MULTI_SIDE_BY_SIDE) {
+    share_sms(m);
+    if ((rc = enqueue_step(m, SHT_MULTI_ROUND_TRIP, m->stream))) return rc;
+    if ((e = cudaStreamSynchronize(m->stream)) != cudaSuccess) return cuda_fail(e, "multi warm-up");
+    if ((rc = check_device_errors(m))) return rc;
+  } else if ((flags & SHT_MULTI_AUTOTUNE) && m->groups.size() > 1 && (rc = tune_partition(m))) {
+    return rc;
+  }
 
   // Capture each step kind: the graph is kept for replay unless the batch
   // runs stage by stage, and the capture counts the kernels of one step.

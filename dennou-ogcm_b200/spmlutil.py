@@ -34,7 +34,7 @@ SHT_OPT_HOST_GRAPHS = 2
 SHT_OPT_HOST_GRAPH_COUNT = 3
 SHT_OPT_LEGENDRE_TILE = 4
 SHT_MULTI_SYNTHESIS, SHT_MULTI_ANALYSIS, SHT_MULTI_ROUND_TRIP = 1, 2, 3
-SHT_MULTI_AUTOTUNE, SHT_MULTI_ALLOW_SPLIT, SHT_MULTI_NO_GRAPH = 1, 2, 4
+SHT_MULTI_AUTOTUNE, SHT_MULTI_ALLOW_SPLIT, SHT_MULTI_NO_GRAPH, SHT_MULTI_SIDE_BY_SIDE = 1, 2, 4, 8
 
 _D = ctypes.POINTER(ctypes.c_double)
 _VP = ctypes.c_void_p
@@ -563,9 +563,10 @@ class MultiTransform:
         self._keep.append((plan, wa, xya))
         return idx.value
 
-    def build(self, autotune: bool = True, allow_split: bool = False, graph: bool = True):
+    def build(self, autotune: bool = True, allow_split: bool = False, graph: bool = True,
+              side_by_side: bool = False):
         flags = (SHT_MULTI_AUTOTUNE if autotune else 0) | (SHT_MULTI_ALLOW_SPLIT if allow_split else 0) | \
-            (0 if graph else SHT_MULTI_NO_GRAPH)
+            (0 if graph else SHT_MULTI_NO_GRAPH) | (SHT_MULTI_SIDE_BY_SIDE if side_by_side else 0)
         _check(self._lib.sht_multi_build(self._h, flags), "sht_multi_build")
 
     def run(self, what: int = SHT_MULTI_ROUND_TRIP):

@@ -392,6 +392,9 @@ typedef struct sht_multi_s sht_multi;
 #define SHT_MULTI_AUTOTUNE 1    /* build: time the Legendre variants per plan, keep the fastest */
 #define SHT_MULTI_ALLOW_SPLIT 2 /* build: the tuner may choose split precision (<= 1e-11 relative) */
 #define SHT_MULTI_NO_GRAPH 4    /* build: launch stage by stage instead of replaying a graph */
+#define SHT_MULTI_SIDE_BY_SIDE 8 /* build: size every group's persistent grids for a share of the SMs
+                                   (in proportion to its tuned time, or its columns untuned) without
+                                   timing the alternative; the autotuner otherwise decides */
 
 /* Creates an empty batch on the current device. */
 SHT_API int sht_multi_create(sht_multi **multi);

@@ -149,6 +149,28 @@ def test_multi_tuner_may_pick_split(plans):
         m.close()
 
 
+@pytest.mark.parametrize("autotune", [False, True])
+def test_multi_side_by_side(plans, autotune):
+    """Groups whose persistent kernels are sized for shares of the SMs (run
+    side by side) give the same results as the single-plan calls and the
+    oracle."""
+    P = pkg()
+    insts = _instances(plans, 9, max_nb=24, seed=29)
+    m = _build(plans, insts, autotune=autotune, side_by_side=True)
+    try:
+        shares = [g["sms"] for g in m.groups()]
+        assert all(s >= 4 for s in shares) and len(shares) > 1, shares
+        m.run(P.SHT_MULTI_ROUND_TRIP)
+        m.synchronize()
+        for x in insts:
+            assert relerr(x["wa"].cpu().numpy(), x["w"]) < 1e-11, x["grid"]
+            ref = x["plan"].xya_wa(torch.from_numpy(x["w"]).cuda())
+            torch.cuda.synchronize()
+            assert relerr(x["xya"].cpu().numpy(), ref.cpu().numpy()) < 1e-12, x["grid"]
+    finally:
+        m.close()
+
+
 def test_multi_argument_errors(plans):
     P = pkg()
     m = P.MultiTransform()
