@@ -205,11 +205,19 @@ struct Unit {
   long long toff;         // table bytes of (m, p)
 };
 
+// Sub-item g = 4 item + sub, item = tile npairs + i: column tile by column
+// tile, and within a tile the band pairs taken alternately from both ends of
+// the list (m = 0, the last pair, m = 1, ...).  A pair (m, N - m) holds N + 4
+// rows, but its cost goes with the number of 64-deep K chunks and 32-row
+// segments of its four sub-items, which is largest for small m; pair-major
+// order had given the CTAs on the first pairs half as much work again as
+// those on the last.
 template <bool INV>
 __device__ __forceinline__ bool setup_sub(const I8Args &a, const Lut &t, int g, Unit &u)
 {
   const int item = g >> 2, sub = g & 3;
-  const int2 pr = t.pairs[item / a.ntiles];
+  const int tile = item / a.npairs, i = item - tile * a.npairs;
+  const int2 pr = t.pairs[(i & 1) ? a.npairs - 1 - (i >> 1) : (i >> 1)];
   if (sub >= 2 && pr.y < 0) return false;
   u.g = g;
   u.m = sub < 2 ? pr.x : pr.y;
@@ -221,7 +229,7 @@ __device__ __forceinline__ bool setup_sub(const I8Args &a, const Lut &t, int g, 
   u.nch = (u.K + kKC - 1) / kKC;
   u.seg = 0;
   u.ch = 0;
-  u.col0 = (item % a.ntiles) * (kM / 2);
+  u.col0 = tile * (kM / 2);
   u.rowoff = t.rowoff[u.m];
   u.toff = t.toff[2 * u.m + u.p];
   u.teoff = t.teoff[2 * u.m + u.p];
