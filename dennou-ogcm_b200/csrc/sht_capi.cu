@@ -165,12 +165,12 @@ void mark(sht_plan *p, int k, cudaStream_t s)
 
 int leg_fwd(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s)
 {
-  if (p->precision == SHT_PREC_SPLIT) return launch_leg_fwd_split(p, F, ncol, S, s);
+  if (use_split(p, true)) return launch_leg_fwd_split(p, F, ncol, S, s);
   return launch_leg_fwd_fp64(p, F, ncol, S, s);
 }
 int leg_inv(sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s)
 {
-  if (p->precision == SHT_PREC_SPLIT) return launch_leg_inv_split(p, S, ncol, F, s);
+  if (use_split(p, false)) return launch_leg_inv_split(p, S, ncol, F, s);
   return launch_leg_inv_fp64(p, S, ncol, F, s);
 }
 
@@ -641,7 +641,7 @@ int check_strided(const sht_plan *p, const void *g, int ldi, int ldj, int nb, co
   int rc = check_plan(p);
   if (rc) return rc;
   if (nb < 0) { set_error("nb must be >= 0"); return SHT_ERR_INVALID_ARG; }
-  if (mode != -1 && mode != SHT_PREC_FP64 && mode != SHT_PREC_SPLIT) {
+  if (mode != -1 && mode != SHT_PREC_FP64 && mode != SHT_PREC_SPLIT && mode != SHT_PREC_AUTO) {
     set_error("unknown precision mode");
     return SHT_ERR_INVALID_ARG;
   }
@@ -902,7 +902,10 @@ int sht_set_precision(sht_plan *p, int mode)
 {
   int rc = check_plan(p);
   if (rc) return rc;
-  if (mode != SHT_PREC_FP64 && mode != SHT_PREC_SPLIT) { set_error("unknown precision mode"); return SHT_ERR_INVALID_ARG; }
+  if (mode != SHT_PREC_FP64 && mode != SHT_PREC_SPLIT && mode != SHT_PREC_AUTO) {
+    set_error("unknown precision mode");
+    return SHT_ERR_INVALID_ARG;
+  }
   std::lock_guard<std::mutex> lk(p->mtx);
   p->precision = mode;
   return SHT_OK;

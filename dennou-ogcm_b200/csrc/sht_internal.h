@@ -180,6 +180,20 @@ int launch_leg_fwd_fp64(const sht_plan *p, const double2 *F, int ncol, double2 *
 int launch_leg_inv_fp64(const sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 
 // --- persistent paired-band FP64 contraction (sht_legendre_v2.cu)
+bool split_supported(const sht_plan *p);
+// Whether a contraction runs in split precision: always under SHT_PREC_SPLIT;
+// under SHT_PREC_AUTO when it is at least 128 terms long (jm/2 latitudes in
+// the analysis, (nm+3)/2 degrees of one parity in the synthesis), where the
+// int8 digit kernel measured faster than the FP64 tensor path on B200 (T170
+// analysis 0.41 against 0.44 ms; T341 3.09 / 2.77 against 3.78 / 3.52 ms; T170
+// synthesis, 86 terms, 0.48 against 0.40 ms).
+inline bool use_split(const sht_plan *p, bool analysis)
+{
+  if (p->precision == SHT_PREC_SPLIT) return true;
+  if (p->precision != SHT_PREC_AUTO || !split_supported(p)) return false;
+  return (analysis ? p->JH : (p->N + 3) / 2) >= 128;
+}
+
 // SMs a plan's persistent kernels size their grids for
 inline int grid_sms(const sht_plan *p)
 {
@@ -199,7 +213,6 @@ int launch_leg_inv_chunk(const sht_plan *p, const double2 *S, int ncol, double2 
 int launch_leg_fwd_split(sht_plan *p, const double2 *F, int ncol, double2 *S, cudaStream_t s);
 int launch_leg_inv_split(sht_plan *p, const double2 *S, int ncol, double2 *F, cudaStream_t s);
 void free_split_tables(sht_plan *p);
-bool split_supported(const sht_plan *p);
 int split_error_status(sht_plan *p);  // reads and clears the device error word (synchronous)
 // one block whose bounded wait runs out on purpose and sets the error word (synchronous)
 int wait_selftest(sht_plan *p, unsigned long long limit_ns);

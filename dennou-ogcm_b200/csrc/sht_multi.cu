@@ -197,7 +197,10 @@ int tune_group(Group &g, bool allow_split)
     cands.push_back({SHT_PREC_FP64, 3, 32});
   }
   cands.push_back({SHT_PREC_FP64, 1, 0});
-  if (allow_split && split_supported(g.plan)) cands.push_back({SHT_PREC_SPLIT, 0, 0});
+  if (allow_split && split_supported(g.plan)) {
+    cands.push_back({SHT_PREC_SPLIT, 0, 0});
+    cands.push_back({SHT_PREC_AUTO, 0, 0});  // split where the contraction is long, FP64 elsewhere
+  }
   float best = 0.f;
   Cand win = cands.front();
   for (const Cand &c : cands) {

@@ -87,7 +87,7 @@ extern "C" SHT_API int sht_wa_xya_dev_noalloc(sht_plan *p, const double *xya, in
     return SHT_ERR_TOO_LARGE;
   }
   std::lock_guard<std::mutex> lk(p->mtx);
-  if (p->precision == SHT_PREC_SPLIT && !p->tc_tables) {
+  if (use_split(p, true) && !p->tc_tables) {
     // the split kernel's digit tables are allocated by the first split-precision
     // transform of a plan; this entry point must not be the one to do it
     set_error("noalloc: split precision needs the plan's digit tables, which the first split-precision "
@@ -107,7 +107,7 @@ extern "C" SHT_API int sht_wa_xya_dev_noalloc(sht_plan *p, const double *xya, in
     double2 *S = reinterpret_cast<double2 *>(static_cast<char *>(base) + fbytes);
     cudaStream_t s = p->stream;
     rc = launch_fft_fwd(p, xya, nullptr, nb, nb, F, nb, 0, RS_FWD_PLAIN, s);
-    if (!rc) rc = (p->precision == SHT_PREC_SPLIT) ? launch_leg_fwd_split(p, F, nb, S, s)
+    if (!rc) rc = use_split(p, true) ? launch_leg_fwd_split(p, F, nb, S, s)
                                                    : launch_leg_fwd_fp64(p, F, nb, S, s);
     if (!rc) rc = launch_pack(p, PACK_PLAIN, S, nb, nb, wa, nullptr, s);
   }

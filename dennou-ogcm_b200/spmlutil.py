@@ -29,6 +29,7 @@ LIB_PATH = os.path.join(_HERE, "libdogcm_sht.so")
 SHT_OK = 0
 SHT_PREC_FP64 = 0
 SHT_PREC_SPLIT = 1
+SHT_PREC_AUTO = 2
 SHT_OPT_LEGENDRE_KERNEL = 1
 SHT_OPT_HOST_GRAPHS = 2
 SHT_OPT_HOST_GRAPH_COUNT = 3

@@ -62,6 +62,11 @@ extern "C" {
                              grid or spectral value, seven per table value),
                              exact integer digit products on the tcgen05
                              tensor cores, FP64 recombination                  */
+#define SHT_PREC_AUTO  2  /* per direction, the faster of the two on B200 as
+                             measured: split precision for a contraction of at
+                             least 128 terms (analysis: jm/2 latitudes;
+                             synthesis: (nm+3)/2 degrees of one parity), FP64
+                             below.  Both meet the same 1e-11 bound.            */
 
 typedef struct sht_plan_s sht_plan;
 
@@ -113,8 +118,8 @@ SHT_API int sht_plan_nm_l(const sht_plan *plan, int l, int *n, int *m);
 /* rn(:,1) (SpmlUtil_mod.f90:135): Laplacian eigenvalue -n(n+1) per l. */
 SHT_API int sht_rn(const sht_plan *plan, double *rn);
 
-/* Precision of the Legendre contraction for the following calls
- * (SHT_PREC_FP64 is the default). */
+/* Precision of the Legendre contraction for the following calls:
+ * SHT_PREC_FP64 (the default), SHT_PREC_SPLIT or SHT_PREC_AUTO. */
 SHT_API int sht_set_precision(sht_plan *plan, int mode);
 SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
 

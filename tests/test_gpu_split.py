@@ -178,3 +178,31 @@ def test_config_full_batch_split_vs_fp64(cfg):
         assert _trel(got["back"], w) < TOL and _trel(ref["back"], w) < TOL
     finally:
         gpu.final()
+
+
+def test_per_direction_precision(plan_cache):
+    """SHT_PREC_AUTO: split precision for a contraction of at least 128 terms
+    (the analysis at jm/2 >= 128, the synthesis at (nm+3)/2 >= 128), FP64 for
+    the others.  T85: both directions as FP64, bit for bit; T170: the analysis
+    as split, the synthesis as FP64, bit for bit, and both against the oracle."""
+    P, W = pkg(), workloads()
+    for I, J, N in ((256, 128, 85), (512, 256, 170)):
+        gpu, ora = plan_cache(I, J, N)
+        rng = np.random.default_rng(N)
+        w = W.seeded_spectra(N, 9, 2.0, rng=rng)
+        x = rng.standard_normal((9, J, I))
+        out = {}
+        try:
+            for mode in (P.SHT_PREC_FP64, P.SHT_PREC_SPLIT, P.SHT_PREC_AUTO):
+                gpu.set_precision(mode)
+                assert gpu.get_precision() == mode
+                out[mode] = (gpu.xya_wa(w), gpu.wa_xya(x))
+        finally:
+            gpu.set_precision(P.SHT_PREC_FP64)
+        syn_split, ana_split = (N + 3) // 2 >= 128, J // 2 >= 128
+        assert np.array_equal(out[P.SHT_PREC_AUTO][0], out[P.SHT_PREC_SPLIT if syn_split else P.SHT_PREC_FP64][0])
+        assert np.array_equal(out[P.SHT_PREC_AUTO][1], out[P.SHT_PREC_SPLIT if ana_split else P.SHT_PREC_FP64][1])
+        assert relerr(out[P.SHT_PREC_AUTO][0], ora.xya_wa(w)) < TOL
+        assert relerr(out[P.SHT_PREC_AUTO][1], ora.wa_xya(x)) < TOL
+    with pytest.raises(P.SpmlError):
+        gpu.set_precision(3)
