@@ -574,7 +574,11 @@ def main():
     # per_direction: SHT_PREC_AUTO, split precision for the contractions of at
     # least 128 terms and FP64 for the others
     PREC = {"fp64": P.SHT_PREC_FP64, "split": P.SHT_PREC_SPLIT, "per_direction": P.SHT_PREC_AUTO}
-    modes = ["fp64", "split", "per_direction"] if args.precision == "auto" else [args.precision]
+    modes = ["fp64", "split"] if args.precision == "auto" else [args.precision]
+    # per_direction differs from both only where one direction is long enough
+    # for split precision and the other is not (T170 here)
+    if args.precision == "auto" and (J // 2 >= 128) != ((N + 3) // 2 >= 128):
+        modes.append("per_direction")
     for mode in modes:
         prec = PREC[mode]
         try:
