@@ -19,7 +19,7 @@ module wa_module_b200
   implicit none
   private
 
-  public :: wa_Initial, wa_Finalize
+  public :: wa_Initial, wa_Finalize, b200_SetPrecision
   public :: x_Lon, y_Lat, x_Lon_Weight, y_Lat_Weight, xy_Lon, xy_Lat
   public :: rn, l_nm, nm_l
   public :: w_xy, xy_w, wa_xya, xya_wa
@@ -40,6 +40,8 @@ module wa_module_b200
   public :: w_Lapla2D_w, wz_Lapla2D_wz, w_InvLapla2D_w, wz_InvLapla2D_wz
 
   integer, parameter :: SHT_OK = 0
+  ! precision modes of the Legendre contraction (include/dogcm_sht.h)
+  integer, parameter, public :: SHT_PREC_FP64 = 0, SHT_PREC_SPLIT = 1, SHT_PREC_AUTO = 2
   character(*), parameter :: module_name = 'wa_module_b200'
 
   type(c_ptr), save :: plan = c_null_ptr
@@ -71,6 +73,11 @@ module wa_module_b200
       type(c_ptr), value :: plan
       real(c_double), intent(out) :: x_lon(*), y_lat(*), x_w(*), y_w(*)
     end function sht_grid_info
+    integer(c_int) function sht_set_precision(plan, mode) bind(C, name='sht_set_precision')
+      import :: c_int, c_ptr
+      type(c_ptr), value :: plan
+      integer(c_int), value :: mode
+    end function sht_set_precision
     integer(c_int) function sht_rn(plan, rnv) bind(C, name='sht_rn')
       import :: c_int, c_double, c_ptr
       type(c_ptr), value :: plan
@@ -271,6 +278,15 @@ contains
     call check(sht_rn(plan, rn(:, 1)), 'wa_Initial')
     rn(:, 2) = 0.0_DP  ! only rn(:,1), the Laplacian eigenvalue, is used by dogcm
   end subroutine wa_Initial
+
+  !> Precision of the following transforms: SHT_PREC_FP64 (the default),
+  !> SHT_PREC_SPLIT (integer digit products on the tensor cores, <= 1e-11
+  !> relative) or SHT_PREC_AUTO (split where a contraction has at least 128
+  !> terms: the faster of the two per direction).  No counterpart in SPMODEL.
+  subroutine b200_SetPrecision(mode)
+    integer, intent(in) :: mode
+    call check(sht_set_precision(plan, int(mode, c_int)), 'SetPrecision')
+  end subroutine b200_SetPrecision
 
   subroutine wa_Finalize()
     if (c_associated(plan)) call check(sht_final(plan), 'wa_Finalize')
