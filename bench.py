@@ -11,7 +11,9 @@ transform is one field-level through both.
          a 256 MiB write between steps, outside the timed events).
   e2e    the same metric through the host-pointer C-ABI (sht_xya_wa then
          sht_wa_xya on pinned host arrays): every step moves the spectra in,
-         the grid out and back, and the spectra out over PCIe.
+         the grid out and back, and the spectra out over PCIe.  Its
+         pcie_floor is the time plain pinned copies of the same bytes take
+         (each call bound by its larger direction), against the measured time.
 
 Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                         [--precision auto|fp64|split|per_direction] [--nb NB]
@@ -671,6 +673,28 @@ def main():
                "h2d_bytes_per_step": 8 * nb * (L + I * J), "d2h_bytes_per_step": 8 * nb * (I * J + L),
                "path": "sht_xya_wa + sht_wa_xya on pinned host arrays (synchronous C-ABI calls, host clock)",
                "relerr": _rel(wo.numpy(), wh.numpy())}
+        # the copy floor: plain pinned copies of the grid batch in each
+        # direction (CUDA events); each call is bound by its larger direction
+        gd = _t.empty((nb, J, I), dtype=_t.float64, device=dev)
+        cs = _t.cuda.Stream()
+        bw = {}
+        for name, dst, src in (("h2d", gd, gh), ("d2h", gh, gd)):
+            with _t.cuda.stream(cs):
+                for _ in range(2):
+                    dst.copy_(src, non_blocking=True)
+                e0, e1 = _t.cuda.Event(enable_timing=True), _t.cuda.Event(enable_timing=True)
+                e0.record(cs)
+                for _ in range(5):
+                    dst.copy_(src, non_blocking=True)
+                e1.record(cs)
+            cs.synchronize()
+            bw[name] = 5 * gd.numel() * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        del gd
+        gb, lb = 8 * nb * I * J, 8 * nb * L
+        floor_ms = 1e3 * (max(lb / bw["h2d"], gb / bw["d2h"]) + max(gb / bw["h2d"], lb / bw["d2h"])) / 1e9
+        e2e["pcie_floor"] = {"copy_gbs": bw, "ms_per_step": floor_ms,
+                             "measured_ms_per_step": 1e3 * el / args.steps,
+                             "frac": floor_ms / (1e3 * el / args.steps)}
 
     multi = None if args.no_multi else bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world)
     fused = None if args.no_fused else bench_fused(P, torch, dev, sht, args, flush, max_over_ranks)

@@ -41,7 +41,6 @@ struct SpecArgs {
   double *o0, *o1;        // pack outputs
   int nb, N, L;
   double radius;
-  const int *rowoff;
   const double *eps;      // [m][n], n = 0..N+2
   const int2 *tiles;      // (n, m0) per tile
   double *const *ocol;        // optional per-field-level pack destinations
@@ -60,6 +59,11 @@ __device__ __forceinline__ double eps_at(const SpecArgs &a, int m, int n)
 {
   return (n < 0 || n > a.N + 2) ? 0.0 : __ldg(a.eps + (long long)m * (a.N + 3) + n);
 }
+
+// Internal row of (m, n): rowoff(m) + n - m, with rowoff(m) = sum over m' < m
+// of the N + 2 - m' rows of band m' (the plan's row table in closed form, so
+// that no dependent load precedes the coefficient loads)
+__device__ __forceinline__ int spec_row(int N, int m, int n) { return m * (N + 2) - m * (m - 1) / 2 + (n - m); }
 __device__ __forceinline__ double2 cadd(double2 x, double2 y) { return make_double2(x.x + y.x, x.y + y.y); }
 __device__ __forceinline__ double2 csub(double2 x, double2 y) { return make_double2(x.x - y.x, x.y - y.y); }
 __device__ __forceinline__ double2 cscale(double2 x, double s) { return make_double2(x.x * s, x.y * s); }
@@ -94,7 +98,7 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   for (int i = 0; i < NI; ++i) {
     const int m = m0 + warp + 8 * i;
     const bool ok = m <= n && m < a.M && b < a.nb;
-    const long long base = ok ? (long long)(__ldg(a.rowoff + m) + (n - m)) * a.ncolS + b : 0;
+    const long long base = ok ? (long long)spec_row(a.N, m, n) * a.ncolS + b : 0;
 #pragma unroll
     for (int dn = -1; dn <= 1; ++dn)
 #pragma unroll
@@ -140,14 +144,17 @@ __global__ void __launch_bounds__(256) k_pack(SpecArgs a)
   __syncthreads();
   // write runs w[b][n(n+1) + m] and w[b][n(n+1) - m]
   const int mi = lane, m = m0 + mi;
-  for (int bi = warp; bi < kBC; bi += 8) {
-    const int bb = b0 + bi;
-    if (bb >= a.nb || m > n || m >= a.M) continue;
+  if (m > n || m >= a.M) return;
+  const long long lc = spml_l(a, n, m, 0), ls = spml_l(a, n, m, 1);
+#pragma unroll
+  for (int q = 0; q < kBC / 8; ++q) {
+    const int bi = warp + 8 * q, bb = b0 + bi;
+    if (bb >= a.nb) break;
 #pragma unroll
     for (int o = 0; o < NOUT; ++o) {
       double *w = (o == 0 && a.ocol) ? a.ocol[bb] : ((o == 0) ? a.o0 : a.o1) + (long long)bb * a.L;
-      w[spml_l(a, n, m, 0)] = out[o][0][mi][bi];
-      if (m > 0) w[spml_l(a, n, m, 1)] = out[o][1][mi][bi];
+      w[lc] = out[o][0][mi][bi];
+      if (m > 0) w[ls] = out[o][1][mi][bi];
     }
   }
 }
@@ -187,19 +194,36 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
   // orders m0..m0+31, both parts).  Warp w takes field-levels b0 + 8i' + w of
   // every run, so the run of each unrolled load is a compile-time constant;
   // all loads of a warp are issued before any of them is stored.
-  constexpr int PER = NIN * 6 * (kBC / 8);
+  constexpr int NQ = kBC / 8;
+  constexpr int PER = NIN * 6 * NQ;
   double val[PER];
   const int m = m0 + lane;
+  // the row of each of this warp's field-levels, and the SPML offset of each
+  // run (-1 where the entry does not exist), formed once for all loads
+  const double *wr[NIN][NQ];
+#pragma unroll
+  for (int in = 0; in < NIN; ++in)
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+      const int bb = b0 + 8 * q + warp;
+      wr[in][q] = bb >= a.nb ? nullptr
+                : (in == 0 && a.icol) ? a.icol[bb] : ((in == 0) ? a.w0 : a.w1) + (long long)bb * a.L;
+    }
+  int off[6];
+#pragma unroll
+  for (int r = 0; r < 6; ++r) {
+    const int nn = n + r / 2 - 1, sn = r & 1;
+    const bool ok = nn >= 0 && nn <= a.N && m <= nn && m < a.M && !(sn && m == 0);
+    off[r] = ok ? (int)spml_l(a, nn, m, sn) : -1;
+  }
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
-    const int run = i / (kBC / 8), in = run / 6, dn = (run % 6) / 2 - 1, sn = run & 1;
+    const int run = i / NQ;
     val[i] = 0.0;
-    if (!unpack_needs<OP>(in, dn)) continue;
-    const int nn = n + dn, bb = b0 + 8 * (i % (kBC / 8)) + warp;
-    if (nn >= 0 && nn <= a.N && m <= nn && m < a.M && bb < a.nb && !(sn && m == 0)) {
-      const double *w = (in == 0 && a.icol) ? a.icol[bb] : ((in == 0) ? a.w0 : a.w1) + (long long)bb * a.L;
-      val[i] = __ldg(w + spml_l(a, nn, m, sn));
-    }
+    if (!unpack_needs<OP>(run / 6, (run % 6) / 2 - 1)) continue;
+    const double *w = wr[run / 6][i % NQ];
+    const int o = off[run % 6];
+    if (w && o >= 0) val[i] = __ldg(w + o);
   }
 #pragma unroll
   for (int i = 0; i < PER; ++i) {
@@ -210,11 +234,11 @@ __global__ void __launch_bounds__(256) k_unpack(SpecArgs a)
   __syncthreads();
   const int b = b0 + lane;
   if (b >= a.nb) return;
-  int rows[kMC / 8];  // row offsets of this warp's orders, loaded before the loop
+  int rows[kMC / 8];  // internal rows of this warp's orders
 #pragma unroll
   for (int i = 0; i < kMC / 8; ++i) {
     const int m = m0 + warp + 8 * i;
-    rows[i] = (m <= n && m <= a.N && m < a.M) ? __ldg(a.rowoff + m) + (n - m) : -1;
+    rows[i] = (m <= n && m <= a.N && m < a.M) ? spec_row(a.N, m, n) : -1;
   }
 #pragma unroll
   for (int i = 0; i < kMC / 8; ++i) {
@@ -324,7 +348,7 @@ int launch_pack(const sht_plan *p, int op, const double2 *S, int ncolS, int nb, 
   a.ocol = wcol;
   a.S = S; a.ncolS = ncolS; a.o0 = w0; a.o1 = w1 ? w1 : w0;
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
-  a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
+  a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
   a.M = p->M; a.zonal = p->zonal ? 1 : 0;
   dim3 grid(p->n_pack_tiles, (nb + kBC - 1) / kBC);
   switch (op) {
@@ -348,7 +372,7 @@ int launch_unpack(const sht_plan *p, int op, const double *w0, const double *w1,
   a.icol = wcol;
   a.So = S; a.ncolS = ncolS; a.w0 = w0; a.w1 = w1 ? w1 : w0;
   a.nb = nb; a.N = p->N; a.L = p->L; a.radius = p->radius;
-  a.rowoff = p->d_rowoff; a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
+  a.eps = p->d_eps; a.tiles = p->d_spec_tiles;
   a.M = p->M; a.zonal = p->zonal ? 1 : 0;
   dim3 grid(p->n_spec_tiles, (nb + kBC - 1) / kBC);
   const size_t one = sizeof(double) * kMC * (kBC + 1);  // one staged run
