@@ -555,11 +555,20 @@ int host_call(sht_plan *p, int op, const double *i0, const double *i1, int nb, d
     if (rc) return rc;
   } else {
     const size_t pin = nin_each / nb, pout = nout_each / nb;  // doubles per field-level
+    // Chunk sizes ramp up and down (weights 1, 2, 3, ..., 3, 2, 1): only the
+    // first chunk's upload and kernels and the last chunk's kernels and
+    // download overlap nothing, so those chunks are the small ones.
+    int wsum = 0, wpre[9] = {0};
+    for (int c = 0; c < nchunk; ++c) {
+      const int w = std::min(std::min(c + 1, nchunk - c), 3);
+      wpre[c + 1] = wpre[c] + w;
+      wsum += w;
+    }
     // the plan stream and the copy streams start after any earlier work on the plan stream
     if ((e = cudaEventRecord(p->chunk_ev[0], s)) != cudaSuccess) return cuda_fail(e, "chunk event");
     if ((e = cudaStreamWaitEvent(p->copy_in, p->chunk_ev[0], 0)) != cudaSuccess) return cuda_fail(e, "chunk wait");
     for (int c = 0; c < nchunk; ++c) {
-      const int b0 = (int)((long long)nb * c / nchunk), b1 = (int)((long long)nb * (c + 1) / nchunk), n = b1 - b0;
+      const int b0 = (int)((long long)nb * wpre[c] / wsum), b1 = (int)((long long)nb * wpre[c + 1] / wsum), n = b1 - b0;
       cudaEvent_t ein = p->chunk_ev[2 * c], eout = p->chunk_ev[2 * c + 1];
       for (int k = 0; k < sh.nin; ++k)
         if ((e = cudaMemcpyAsync(din[k] + b0 * pin, hin[k] + b0 * pin, sizeof(double) * n * pin,
