@@ -23,6 +23,8 @@
 #include "sht_internal.h"
 #include "sht_l2.cuh"
 
+#include <type_traits>
+
 namespace sht {
 
 // cos(pi q / 16), q = 0..8 (standard constants to 32 significant digits)
@@ -315,15 +317,17 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
   constexpr int JTh = JT / 2;
   const int tid = threadIdx.x, r = tid / T, u = tid % T;
   const int ntile = (a.JH + JTh - 1) / JTh;
-  const long long ntot = (long long)a.ncol * ntile;
+  // tile indices fit in 32 bits (the launcher checks), so the per-tile
+  // division is a 32-bit one
+  const unsigned ntot = (unsigned)a.ncol * (unsigned)ntile;
   const long long IJ = (long long)a.I * a.J;
   // tile t -> (column, first row pair); this thread's row j and whether it exists
-  auto where = [&](long long t, int &col, int &h0, int &j, bool &valid) {
+  auto where = [&](unsigned t, int &col, int &h0, int &j, bool &valid) {
     // last column first: when a synthesis has just written the grid, its
     // last columns are the likeliest to be still in L2
     t = ntot - 1 - t;
-    const int c2 = (int)(t / ntile);
-    h0 = (int)(t - (long long)c2 * ntile) * JTh;
+    const int c2 = (int)(t / (unsigned)ntile);
+    h0 = (int)(t - (unsigned)c2 * (unsigned)ntile) * JTh;
     col = a.mul_pair ? (c2 >> 1) + (c2 & 1) * a.nsplit : c2;
     const int jh = h0 + (r % JTh);
     j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
@@ -338,7 +342,7 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
     // The rows of the block's next tile are loaded into registers before
     // this tile is transformed, so their DRAM latency overlaps the DFTs
     // (not at 32-point first passes, where the second set would spill).
-    long long t = blockIdx.x;
+    unsigned t = blockIdx.x;
     double2 v[R1];
     if (t < ntot) {
       int col, h0, j; bool valid;
@@ -349,7 +353,7 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
     }
     for (; t < ntot; t += gridDim.x) {
       double2 vn[R1];
-      const long long tn = t + gridDim.x;
+      const unsigned tn = t + gridDim.x;
       if (tn < ntot) {
         int coln, h0n, jn; bool validn;
         where(tn, coln, h0n, jn, validn);
@@ -366,7 +370,7 @@ __global__ void __launch_bounds__(NT) k_fft_fwd(FftArgs a)
     }
     return;
   }
-  for (long long t = blockIdx.x; t < ntot; t += gridDim.x) {
+  for (unsigned t = blockIdx.x; t < ntot; t += gridDim.x) {
     int col, h0, j; bool valid;
     where(t, col, h0, j, valid);
     const double2 *src = row_src(col, j, valid);
@@ -413,19 +417,26 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
   constexpr int JTh = JT / 2;  // mirrored row pairs per tile
   const int tid = threadIdx.x, r = tid / T, u = tid % T;
   const int ntile = (a.JH + JTh - 1) / JTh;
-  const long long ntot = (long long)a.ncol * ntile;
+  // Tile indices fit in 32 bits (the launcher checks).  Up to 16-point first
+  // passes the per-tile division is a 32-bit one (T85 / T170 inverse 1-4 %
+  // faster); at 32 points, where the kernel sits at the 255-register cap, the
+  // 64-bit form measured faster (T341 inverse 1.58 against 1.84 ms).
+  using Idx = typename std::conditional<(A <= 4), unsigned, long long>::type;
+  const Idx ntot = (Idx)a.ncol * (Idx)ntile;
   const long long mstride = (long long)a.ncolF * a.J;
 
   // rows [0, JTh) of a staged tile take E (then north), rows [JTh, JT) take O (then south)
-  auto issue = [&](long long t, double2 *buf) {
-    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
+  auto issue = [&](Idx t, double2 *buf) {
+    const int col = (int)(t / (Idx)ntile), h0 = (int)(t - (Idx)col * (Idx)ntile) * JTh;
     const double2 *Fb = a.Fc + (long long)(a.colF0 + col) * a.J + h0;
     const int nh = min(JTh, a.JH - h0);
-    for (int idx = tid; idx < (a.N + 1) * JT; idx += NT) {
-      const int m = idx / JT, rr = idx - m * JT, i = rr % JTh;
-      const bool in = i < nh;
-      cp_async16(buf + m * JTp + rr, in ? Fb + m * mstride + (rr < JTh ? 0 : a.JH) + i : Fb, in);
-    }
+    // NT is a multiple of JT: this thread keeps staged row rr and steps the orders
+    constexpr int MS = NT / JT;
+    const int rr = tid % JT, i = rr % JTh;
+    const bool in = i < nh;
+    const double2 *src = Fb + (rr < JTh ? 0 : a.JH) + i + (long long)(tid / JT) * mstride;
+    for (int m = tid / JT; m <= a.N; m += MS, src += MS * mstride)
+      cp_async16(buf + m * JTp + rr, in ? src : Fb, in);
   };
 
   // Up to 16-point first passes the next tile's runs stream into the second
@@ -435,7 +446,7 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
   // complex points (I = 256) one buffer and a 128-register cap give 4 blocks
   // per SM instead of 3 (inverse 55.0 -> 53.9 us at T85, 480 field-levels).
   constexpr bool kDB = A <= 4 && !(A == 4 && B == 3);
-  long long t = blockIdx.x;
+  Idx t = blockIdx.x;
   if (t < ntot) issue(t, sm);
   cp_async_commit();
   for (int it = 0; t < ntot; t += gridDim.x, ++it) {
@@ -449,7 +460,7 @@ __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftA
     }
     __syncthreads();
 
-    const int col = (int)(t / ntile), h0 = (int)(t - (long long)col * ntile) * JTh;
+    const int col = (int)(t / (Idx)ntile), h0 = (int)(t - (Idx)col * (Idx)ntile) * JTh;
     const int jh = h0 + (r % JTh), j = r < JTh ? a.JH + jh : a.JH - 1 - jh;
     const bool valid = jh < a.JH;
 
@@ -769,6 +780,7 @@ int run_fft(bool inverse, const sht_plan *p, const FftArgs &a, cudaStream_t s)
   const size_t smem = sizeof(double2) * (2 * (size_t)S::NC + (inverse && A <= 4 && !(A == 4 && B == 3) ? 2 : 1) * (size_t)bufe);
   const long long ntiles = (long long)a.ncol * ((p->JH + S::JT / 2 - 1) / (S::JT / 2));
   if (ntiles <= 0) return SHT_OK;
+  if (ntiles > 0x7fffffffLL) { set_error("fft: too many field-levels for one call"); return SHT_ERR_TOO_LARGE; }
   if (smem > 227 * 1024) { set_error("fft: shared-memory tile too large for this truncation"); return SHT_ERR_UNSUPPORTED_SIZE; }
   cudaError_t e = cudaSuccess;
   auto go = [&](auto kern, auto... extra) {
