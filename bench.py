@@ -295,7 +295,8 @@ def bench_multi(P, W, torch, dev, args, flush, max_over_ranks, world):
                      "graph_launches_per_step": 1, "build_s": build_s, "relerr": err,
                      "groups": [{"grid": g, "field_levels": x["ncol"], "precision": names[x["precision"]],
                                  "legendre_kernel": {0: "auto", 1: "per-band", 2: "paired persistent",
-                                                     3: "latitude-chunked persistent"}
+                                                     3: "latitude-chunked persistent",
+                                                     4: "single-kernel small-grid transform"}
                                  [x["legendre_kernel"]], "legendre_tile": x["legendre_tile"], "sms": x["sms"],
                                  "tuned_round_trip_ms": x["tuned_ms"]}
                                 for g, x in zip(sorted(grids, key=lambda g: plans[g]._h.value), m.groups())]}

@@ -195,10 +195,17 @@ int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const doubl
                  const double *add1 = nullptr)
 {
   const int nin = g1 ? 2 : 1, ncol = nin * nb;
-  Workspace ws;
-  int rc = ensure_ws(p, ncol, 0, &ws);
-  if (rc) return rc;
   cudaStream_t s = p->stream;
+  int rc;
+  if (pack_op == PACK_PLAIN && rs == RS_FWD_PLAIN && !g1 && !mul && use_small(p, true)) {
+    // one kernel: the stage marks all fall around it (timed as the longitude stage)
+    mark(p, 0, s);
+    if ((rc = launch_small_fwd(p, g0, nullptr, nb, w0, nullptr, s))) return rc;
+    mark(p, 1, s); mark(p, 2, s); mark(p, 3, s);
+    return SHT_OK;
+  }
+  Workspace ws;
+  if ((rc = ensure_ws(p, ncol, 0, &ws))) return rc;
   mark(p, 0, s);
   if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s, nullptr, mul, nb, add0, add1))) return rc;
   mark(p, 1, s);
@@ -214,10 +221,17 @@ int run_synthesis(sht_plan *p, int unpack_op, int rs, const double *w0, const do
                   double *g0, double *g1)
 {
   const int nout = g1 ? 2 : 1, ncol = nout * nb;
-  Workspace ws;
-  int rc = ensure_ws(p, ncol, 0, &ws);
-  if (rc) return rc;
   cudaStream_t s = p->stream;
+  int rc;
+  if (unpack_op == UNPACK_PLAIN && rs == RS_INV_PLAIN && !w1 && !g1 && use_small(p, false)) {
+    // one kernel: the stage marks all fall around it (timed as the longitude stage)
+    mark(p, 0, s); mark(p, 1, s); mark(p, 2, s);
+    if ((rc = launch_small_inv(p, w0, nullptr, nb, g0, nullptr, s))) return rc;
+    mark(p, 3, s);
+    return SHT_OK;
+  }
+  Workspace ws;
+  if ((rc = ensure_ws(p, ncol, 0, &ws))) return rc;
   mark(p, 0, s);
   if ((rc = launch_unpack(p, unpack_op, w0, w1, nb, ws.S, ncol, s))) return rc;
   mark(p, 1, s);
@@ -629,6 +643,7 @@ int run_analysis_cols(sht_plan *p, const double *const *gcol, int ncol, double *
                       double2 *S, cudaStream_t s)
 {
   int rc;
+  if (use_small(p, true)) return launch_small_fwd(p, nullptr, gcol, ncol, nullptr, wcol, s);
   if ((rc = launch_fft_fwd(p, nullptr, nullptr, ncol, ncol, F, ncol, 0, RS_FWD_PLAIN, s, gcol))) return rc;
   if ((rc = leg_fwd(p, F, ncol, S, s))) return rc;
   return launch_pack(p, PACK_PLAIN, S, ncol, ncol, nullptr, nullptr, s, wcol);
@@ -638,6 +653,7 @@ int run_synthesis_cols(sht_plan *p, const double *const *wcol, int ncol, double 
                        double2 *S, cudaStream_t s)
 {
   int rc;
+  if (use_small(p, false)) return launch_small_inv(p, nullptr, wcol, ncol, nullptr, gcol, s);
   if ((rc = launch_unpack(p, UNPACK_PLAIN, nullptr, nullptr, ncol, S, ncol, s, wcol))) return rc;
   if ((rc = leg_inv(p, S, ncol, F, s))) return rc;
   return launch_fft_inv(p, F, ncol, 0, ncol, nullptr, nullptr, ncol, RS_INV_PLAIN, s, gcol);
@@ -936,7 +952,7 @@ int sht_set_option(sht_plan *p, int option, int value)
   std::lock_guard<std::mutex> lk(p->mtx);
   switch (option) {
   case SHT_OPT_LEGENDRE_KERNEL:
-    if (value < 0 || value > 3) { set_error("legendre kernel option must be 0, 1, 2 or 3"); return SHT_ERR_INVALID_ARG; }
+    if (value < 0 || value > 4) { set_error("legendre kernel option must be 0, 1, 2, 3 or 4"); return SHT_ERR_INVALID_ARG; }
     p->leg_kernel = value;
     return SHT_OK;
   case SHT_OPT_LEGENDRE_TILE:

@@ -91,7 +91,8 @@ struct sht_plan_s {
   bool direct_dft = false;  // im not a power of two: longitude transform by direct summation
   int M = 0;           // orders transformed: N + 1, or 1 for a zonal plan
   int precision = SHT_PREC_FP64;
-  int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent
+  int leg_kernel = 0;  // SHT_OPT_LEGENDRE_KERNEL: 0 auto, 1 per-band, 2 paired persistent, 3 latitude-chunked persistent,
+                       // 4 single-kernel small-grid transform (plain analysis and synthesis, im <= 128)
   int leg_tile = 0;    // SHT_OPT_LEGENDRE_TILE: 0 auto; paired kernels: analysis columns per item (8, 16); chunked kernels: latitudes per chunk (16, 32)
 
   // device tables
@@ -187,11 +188,26 @@ bool split_supported(const sht_plan *p);
 // int8 digit kernel measured faster than the FP64 tensor path on B200 (T170
 // analysis 0.41 against 0.44 ms; T341 3.09 / 2.77 against 3.78 / 3.52 ms; T170
 // synthesis, 86 terms, 0.48 against 0.40 ms).
+// --- whole plain transforms of small grids in one kernel (sht_small.cu)
+bool small_supported(const sht_plan *p);
+int launch_small_fwd(const sht_plan *p, const double *g, const double *const *gcol, int ncol, double *w,
+                     double *const *wcol, cudaStream_t s);
+int launch_small_inv(const sht_plan *p, const double *w, const double *const *wcol, int ncol, double *g,
+                     double *const *gcol, cudaStream_t s);
+
 inline bool use_split(const sht_plan *p, bool analysis)
 {
   if (p->precision == SHT_PREC_SPLIT) return true;
   if (p->precision != SHT_PREC_AUTO || !split_supported(p)) return false;
   return (analysis ? p->JH : (p->N + 3) / 2) >= 128;
+}
+
+// plain analysis / synthesis by the single-kernel small-grid transform:
+// chosen with SHT_OPT_LEGENDRE_KERNEL = 4, in FP64 (split precision keeps
+// the batched path)
+inline bool use_small(const sht_plan *p, bool analysis)
+{
+  return p->leg_kernel == 4 && !use_split(p, analysis) && small_supported(p);
 }
 
 // SMs a plan's persistent kernels size their grids for

@@ -185,7 +185,8 @@ int tune_group(Group &g, bool allow_split)
 {
   // kernel families and their tiles: analysis columns per item of the paired
   // kernels, latitudes per chunk of the chunked kernels (a tile a kernel
-  // cannot take falls back to its automatic one and is timed again harmlessly)
+  // cannot take falls back to its automatic one and is timed again
+  // harmlessly), and the single-kernel transform of small grids
   struct Cand { int precision, leg_kernel, leg_tile; };
   std::vector<Cand> cands;
   if (leg_pair_supported(g.plan)) {
@@ -197,6 +198,7 @@ int tune_group(Group &g, bool allow_split)
     cands.push_back({SHT_PREC_FP64, 3, 32});
   }
   cands.push_back({SHT_PREC_FP64, 1, 0});
+  if (small_supported(g.plan)) cands.push_back({SHT_PREC_FP64, 4, 0});  // one kernel per direction
   if (allow_split && split_supported(g.plan)) {
     cands.push_back({SHT_PREC_SPLIT, 0, 0});
     cands.push_back({SHT_PREC_AUTO, 0, 0});  // split where the contraction is long, FP64 elsewhere

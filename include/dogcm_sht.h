@@ -126,8 +126,12 @@ SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
 /* Kernel choices (used by the autotuner and the tests; the defaults are
  * picked per grid).  SHT_OPT_LEGENDRE_KERNEL: 0 automatic, 1 per-band kernel
  * (any grid), 2 persistent paired-band kernel (T85 and smaller), 3 persistent
- * latitude-chunked paired-band kernel (jm/2 a multiple of 16, up to T341).
- * A choice that does not cover the grid falls back to the automatic one. */
+ * latitude-chunked paired-band kernel (jm/2 a multiple of 16, up to T341),
+ * 4 the whole plain analysis or synthesis (w_xy, xy_w and their batched
+ * forms) in one kernel per call, Fourier coefficients kept on chip (power-of-
+ * two im <= 128, jm/2 a multiple of 4, FP64; other operators keep the
+ * automatic kernels).  A choice that does not cover the grid falls back to
+ * the automatic one. */
 #define SHT_OPT_LEGENDRE_KERNEL 1
 /* SHT_OPT_HOST_GRAPHS: 1 (default) replays small host-pointer calls (those
  * staged through the plan's page-locked buffer) as CUDA graphs from the
