@@ -114,6 +114,19 @@ def test_graphs_per_precision_and_kernel_choice():
             sd.set_option(P.SHT_OPT_LEGENDRE_KERNEL, kern)
             for _ in range(3):
                 assert np.array_equal(sg.w_xy(x), sd.w_xy(x)), kern
+        # the single-kernel small-grid transform replays as a graph as well
+        tg, td = _plan(64, 32, 21, True), _plan(64, 32, 21, False)
+        try:
+            y = rng.standard_normal((32, 64))
+            for s_ in (tg, td):
+                s_.set_option(P.SHT_OPT_LEGENDRE_KERNEL, 4)
+            for _ in range(3):
+                assert np.array_equal(tg.w_xy(y), td.w_xy(y))
+                assert np.array_equal(tg.xy_w(tg.w_xy(y)), td.xy_w(td.w_xy(y)))
+            assert tg.get_option(P.SHT_OPT_HOST_GRAPH_COUNT) > 0
+        finally:
+            tg.final()
+            td.final()
         # switching the option off keeps results and stops new captures
         sg.set_option(P.SHT_OPT_HOST_GRAPHS, 0)
         n = sg.get_option(P.SHT_OPT_HOST_GRAPH_COUNT)
