@@ -163,3 +163,27 @@ def test_option_arguments():
             s.set_option(P.SHT_OPT_HOST_GRAPH_COUNT, 0)
     finally:
         s.final()
+
+
+@pytest.mark.parametrize("nb", [97, 250, 385])
+def test_pipelined_host_calls_match_device_calls(nb):
+    """Host-pointer batches of 96 field-levels and more run as a pipeline of
+    2 to 8 chunks of ramped sizes (upload, kernels and download on three
+    streams): every field-level equals the device-pointer call's bit for bit,
+    for an analysis, a synthesis and a two-output operator."""
+    import torch
+
+    s = _plan(128, 64, 42, True)
+    try:
+        rng = np.random.default_rng(nb)
+        x = rng.standard_normal((nb, 64, 128))
+        y = rng.standard_normal((nb, 64, 128))
+        w = s.xya_wa(s.wa_xya(x))  # band-limited spectra
+        xd, yd, wd = (torch.from_numpy(a).cuda() for a in (x, y, w))
+        assert np.array_equal(s.wa_xya(x), s.wa_xya(xd).cpu().numpy())
+        assert np.array_equal(s.xya_wa(w), s.xya_wa(wd).cpu().numpy())
+        vh, dh = s.calc_UVCosLat2VorDiv(x, y)
+        vd, dd = s.calc_UVCosLat2VorDiv(xd, yd)
+        assert np.array_equal(vh, vd.cpu().numpy()) and np.array_equal(dh, dd.cpu().numpy())
+    finally:
+        s.final()
