@@ -140,7 +140,7 @@ template <int A, int B, int NT>
 __global__ void __launch_bounds__(NT, (A == 4 && B == 3) ? 4 : 1) k_fft_inv(FftArgs a, int bufe)
 {
   using S = FftShape<A, B, NT>;
-  constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT, RS = S::RS, JTp = S::JTp;
+  constexpr int R1 = S::R1, R2 = S::R2, NC = S::NC, T = S::T, JT = S::JT, JTp = S::JTp;
   constexpr int NS = R1 / T;
   extern __shared__ __align__(16) double2 smem_all[];
   double2 *stw = smem_all, *stwI = smem_all + NC, *sm = smem_all + 2 * NC;
