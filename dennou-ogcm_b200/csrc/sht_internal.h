@@ -203,11 +203,14 @@ inline bool use_split(const sht_plan *p, bool analysis)
 }
 
 // plain analysis / synthesis by the single-kernel small-grid transform:
-// chosen with SHT_OPT_LEGENDRE_KERNEL = 4, in FP64 (split precision keeps
-// the batched path)
+// chosen with SHT_OPT_LEGENDRE_KERNEL = 4, and by the automatic choice for
+// im = 32 (16 complex points per row), the only size where it measured
+// faster than the batched kernels (T10, 480 field-levels: round trip 31
+// against 59 us); in FP64 only (split precision keeps the batched path)
 inline bool use_small(const sht_plan *p, bool analysis)
 {
-  return p->leg_kernel == 4 && !use_split(p, analysis) && small_supported(p);
+  const bool want = p->leg_kernel == 4 || (p->leg_kernel == 0 && p->NC == 16);
+  return want && !use_split(p, analysis) && small_supported(p);
 }
 
 // SMs a plan's persistent kernels size their grids for

@@ -130,8 +130,8 @@ SHT_API int sht_get_precision(const sht_plan *plan, int *mode);
  * 4 the whole plain analysis or synthesis (w_xy, xy_w and their batched
  * forms) in one kernel per call, Fourier coefficients kept on chip (power-of-
  * two im <= 128, jm/2 a multiple of 4, FP64; other operators keep the
- * automatic kernels).  A choice that does not cover the grid falls back to
- * the automatic one. */
+ * automatic kernels; the automatic choice for im = 32).  A choice that does
+ * not cover the grid falls back to the automatic one. */
 #define SHT_OPT_LEGENDRE_KERNEL 1
 /* SHT_OPT_HOST_GRAPHS: 1 (default) replays small host-pointer calls (those
  * staged through the plan's page-locked buffer) as CUDA graphs from the

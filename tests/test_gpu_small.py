@@ -57,7 +57,8 @@ def test_small_matches_batched_and_oracle(grid, nb, plans):
     I, J, N = grid
     gpu, ora = plans(I, J, N)
     w, x = _inputs(I, J, N, nb, seed=31 + nb)
-    ref = _with_kernel(gpu, 0, lambda: (gpu.xya_wa(w), gpu.wa_xya(x)))
+    # the per-band kernel family (1) keeps the batched path on every grid
+    ref = _with_kernel(gpu, 1, lambda: (gpu.xya_wa(w), gpu.wa_xya(x)))
     got = _with_kernel(gpu, 4, lambda: (gpu.xya_wa(w), gpu.wa_xya(x)))
     assert relerr(got[0], ref[0]) < 1e-13
     assert relerr(got[1], ref[1]) < 1e-13
@@ -159,3 +160,17 @@ def test_small_in_multi_instance_batches(plans):
     finally:
         for p in own.values():
             p.final()
+
+
+def test_small_is_the_automatic_choice_at_im_32(plans):
+    """im = 32 (T10) takes the single kernel by default: one launch per call."""
+    P = pkg()
+    gpu, ora = plans(32, 16, 10)
+    w, x = _inputs(32, 16, 10, 12, seed=3)
+    wd = torch.from_numpy(w).cuda()
+    torch.cuda.synchronize()
+    n0 = P.launch_count()
+    g = gpu.xya_wa(wd)
+    torch.cuda.synchronize()
+    assert P.launch_count() - n0 == 1
+    assert relerr(g.cpu().numpy(), ora.xya_wa(w)) < TOL
