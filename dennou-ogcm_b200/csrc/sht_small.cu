@@ -322,6 +322,17 @@ int run_small(bool inverse, const sht_plan *p, SmallArgs a, cudaStream_t s)
   return e == cudaSuccess ? SHT_OK : cuda_fail(e, inverse ? "k_small_inv" : "k_small_fwd");
 }
 
+// shared memory of the larger of the two directions' blocks on this plan
+template <int A, int B>
+size_t small_smem(const sht_plan *p)
+{
+  using C = SmallCfg<A, B>;
+  using Sh = SmallShape<A, B, C::NT, C::G>;
+  const int bufe = FftShape<A, B, C::NT>::buf_elems(p->N);
+  const size_t f = Sh::smem_fwd(p->N, p->J, bufe), i = Sh::smem_inv(p->N, p->J, bufe);
+  return f > i ? f : i;
+}
+
 int dispatch_small(bool inverse, const sht_plan *p, const SmallArgs &a, cudaStream_t s)
 {
   switch (p->NC) {
@@ -347,8 +358,16 @@ SmallArgs small_args(const sht_plan *p, int ncol, int rs)
 
 bool small_supported(const sht_plan *p)
 {
-  return !p->zonal && !p->direct_dft && (p->NC == 16 || p->NC == 32 || p->NC == 64) && p->JH % 4 == 0 &&
-         p->JH <= 64 && p->N + 1 <= p->NC;
+  if (p->zonal || p->direct_dft || p->JH % 4 != 0 || p->JH > 64 || p->N + 1 > p->NC) return false;
+  // the group's Fourier arrays must fit in one block's shared memory (not so
+  // for, e.g., im = 128 with jm = 128 and nm = 63)
+  const size_t lim = 227 * 1024;
+  switch (p->NC) {
+  case 16: return small_smem<2, 2>(p) <= lim;
+  case 32: return small_smem<3, 2>(p) <= lim;
+  case 64: return small_smem<3, 3>(p) <= lim;
+  default: return false;
+  }
 }
 
 int launch_small_fwd(const sht_plan *p, const double *g, const double *const *gcol, int ncol, double *w,

@@ -115,8 +115,9 @@ def test_small_falls_back_elsewhere(plans):
         assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
     finally:
         gpu.set_precision(P.SHT_PREC_FP64)
-    # grids the single kernel does not take: T85 and a longitude count with a factor of 3
-    for I, J, N in ((256, 128, 85), (96, 48, 31)):
+    # grids the single kernel does not take: T85, a longitude count with a
+    # factor of 3, and a grid whose Fourier arrays exceed a block's shared memory
+    for I, J, N in ((256, 128, 85), (96, 48, 31), (128, 128, 63)):
         gpu, _ = plans(I, J, N)
         w, x = _inputs(I, J, N, 4, seed=9)
         a = _with_kernel(gpu, 0, lambda: (gpu.xya_wa(w), gpu.wa_xya(x)))
