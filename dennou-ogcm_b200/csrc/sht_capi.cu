@@ -204,7 +204,7 @@ int run_analysis(sht_plan *p, int pack_op, int rs, const double *g0, const doubl
     mark(p, 1, s); mark(p, 2, s); mark(p, 3, s);
     return SHT_OK;
   }
-  Workspace ws;
+  Workspace ws{};
   if ((rc = ensure_ws(p, ncol, 0, &ws))) return rc;
   mark(p, 0, s);
   if ((rc = launch_fft_fwd(p, g0, g1, nb, ncol, ws.F, ncol, 0, rs, s, nullptr, mul, nb, add0, add1))) return rc;
@@ -230,7 +230,7 @@ int run_synthesis(sht_plan *p, int unpack_op, int rs, const double *w0, const do
     mark(p, 3, s);
     return SHT_OK;
   }
-  Workspace ws;
+  Workspace ws{};
   if ((rc = ensure_ws(p, ncol, 0, &ws))) return rc;
   mark(p, 0, s);
   if ((rc = launch_unpack(p, unpack_op, w0, w1, nb, ws.S, ncol, s))) return rc;
@@ -286,14 +286,14 @@ int run_dev(sht_plan *p, int op, const double *i0, const double *i1, int nb, dou
   case OP_HGRAD_G: {
     // the spectra stay in the workspace temp, sized for both steps up front
     // so that neither step reallocates under it
-    Workspace ws;
+    Workspace ws{};
     int rc = ensure_ws(p, 2 * nb, nb, &ws);
     if (rc) return rc;
     if ((rc = run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, i0, nullptr, nb, ws.W, nullptr))) return rc;
     return run_synthesis(p, UNPACK_HGRAD, RS_INV_INVCOS, ws.W, nullptr, nb, o0, o1);
   }
   case OP_FLUXDIV_G: {
-    Workspace ws;
+    Workspace ws{};
     int rc = ensure_ws(p, 2 * nb, nb, &ws);
     if (rc) return rc;
     if ((rc = run_analysis(p, PACK_ALPHA, RS_FWD_INV1MMU2, i0, i1, nb, ws.W, nullptr))) return rc;
@@ -1231,7 +1231,7 @@ int sht_roundtrip_diffuse_dev(sht_plan *p, double *xya, int nb, const double *co
   std::lock_guard<std::mutex> lk(p->mtx);
   DeviceGuard g(p->device);
   if (!g.ok) { set_error("cudaSetDevice failed"); return SHT_ERR_CUDA; }
-  Workspace ws;
+  Workspace ws{};
   if ((rc = ensure_ws(p, nb, nb, &ws))) return rc;
   if ((rc = run_analysis(p, PACK_PLAIN, RS_FWD_PLAIN, xya, nullptr, nb, ws.W, nullptr))) return rc;
   if (coef && (rc = launch_diffuse(p, ws.W, nb, coef, dt, filter, p->stream))) return rc;
