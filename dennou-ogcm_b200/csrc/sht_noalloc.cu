@@ -7,9 +7,11 @@
 // cannot afford the implicit device-wide synchronisation cudaMalloc/cudaFree
 // can perform in the middle of a timestep.  Another is a host whose policy
 // forbids allocation after start-up.  For them, sht_wa_xya_dev_noalloc runs
-// the same kernels as sht_wa_xya_dev.  Its intermediate Fourier and spectral
-// arrays live in one fixed, file-scope device array instead of the plan's
-// growable workspace.  The plan itself (Gauss and Legendre tables) is still
+// the batched kernels of sht_wa_xya_dev (longitude transform, contraction,
+// spectral conversion; at im = 32, where sht_wa_xya_dev takes its single
+// fused kernel instead, the two agree to rounding).  Its intermediate Fourier
+// and spectral arrays live in one fixed, file-scope device array instead of
+// the plan's growable workspace.  The plan itself (Gauss and Legendre tables) is still
 // built by sht_init beforehand.
 //
 // Rules a user must know:
